@@ -1,0 +1,1708 @@
+/*
+ * AGBNP3 energy + gradient on the GPU.
+ *
+ * One evaluation of the reference's agbnp3_total_energy()
+ * (agbnp3.c:1221-1816) as a fixed sequence of kernels over a device system
+ * of one or more concatenated instances:
+ *
+ *   prep      gather coordinates to internal order, reset accumulators
+ *   nblist    heavy-atom near list via a hashed cell grid: count -> scan ->
+ *             emit, each list sorted by (float d^2, index)  (agbnp3.c:3978-4115)
+ *   volumes   overlap tree, orders 2..5, level-synchronous count -> scan ->
+ *             emit; kept overlaps are stored once and reused by the
+ *             derivative pass  (agbnp3_cpu_simd_kernels.c:1064-1598)
+ *   scaling   scaling factors, filtered areas, cavity energy
+ *             (agbnp3_utils.c:524-613)
+ *   invb      descreening integrals -> inverse Born radii -> Born radii,
+ *             vdW energy  (agbnp3_cpu_simd_kernels.c:500-678,
+ *             agbnp3_utils.c:615-670, agbnp3.c:1466-1487)
+ *   agb       GB pair energy, gradient at constant Born radii, A_i
+ *             (agbnp3_cpu_simd_kernels.c:66-151, 329-460)
+ *   gbders    gradient through the Born radii at constant self volumes and
+ *             U_i / V_i  (agbnp3_cpu_simd_kernels.c:681-904)
+ *   ws        water sites, free volumes, HB energy and gradient
+ *             (agbnp3.c:1837-3761, agbnp3_cpu_simd_kernels.c:2637-2954)
+ *   treeders  self-volume and surface-area derivatives over every kept
+ *             overlap  (agbnp3_cpu_simd_kernels.c:1601-2405)
+ *   final     outputs to caller order, per-instance energy sums
+ *
+ * The pair and overlap arithmetic is templated on R: double for the plain
+ * FP64 path, float for the mixed path.  Every accumulation (Born-radius
+ * descreening sums, inclusion-exclusion volume and area sums, gradients,
+ * energies) is double in both.  No index is ever produced by an atomic:
+ * sizes come from count -> exclusive scan -> emit.
+ */
+#include "agbnp3_launch.cuh"
+#include "agbnp3_dev.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* model constants (agbnp3_private.h:88-137, 680-684; agbnp3.c:1230-1235) */
+#define C_PI 3.14159265359
+#define C_KFC 2.5
+#define C_PFC 2.97354
+#define C_VOLA 0.01
+#define C_VOLB 0.1
+#define C_RINC 0.5
+#define C_HBRAD 1.4
+#define C_HBLEN 2.5
+#define C_HBSWA 0.65
+#define C_HBSWB 1.0
+#define C_HBSWA0 0.6
+#define C_RW 1.4
+#define C_TOKCAL 332.0
+#define C_AMAX 20.0
+#define WS_MAXC 256 /* heavy atoms within a water site's search radius */
+
+#define BLK 128
+
+struct __align__(16) f4 {
+  float x, y, z, w;
+};
+
+/* ------------------------------------------------------------------------ */
+/* device view: every pointer a kernel may need                             */
+/* ------------------------------------------------------------------------ */
+struct View {
+  int ninst, natoms, nws, ntypes, compat;
+  const int *inst_begin, *inst_nheavy, *inst_of, *ws_begin, *ws_inst;
+  const double *inst_df;
+  const float *inst_cell;
+  const int *bucket_begin, *bucket_mask;
+  const int *ext_of;
+  const double *r, *charge, *igamma, *sgamma, *ialpha, *salpha, *vols;
+  const int *rtype;
+  const double *tab_d;
+  const float *tab_f;
+  const int *ws_kind, *ws_parent, *ws_nparent, *ws_prev;
+  const double *ws_khb;
+  /* per evaluation */
+  const double *x_ext, *y_ext, *z_ext;
+  f4 *pos;
+  double *pxd, *pyd, *pzd;
+  int *atom_cell, *atom_bucket;
+  int *bucket_count, *bucket_start, *bucket_cursor, *cell_atoms;
+  int *nl_count, *nl_off, *nl_list;
+  float *nl_d2;
+  int cap_nl;
+  int cap[AGB_MAX_ORDER + 1];
+  int *lv_cnt[AGB_MAX_ORDER + 1], *lv_off[AGB_MAX_ORDER + 1];
+  int *par[AGB_MAX_ORDER + 1], *gend[AGB_MAX_ORDER + 1];
+  void *rec[AGB_MAX_ORDER + 1];
+  int *dc; /* device counters, DC_* */
+  double *volumep, *surf, *surf_f, *sp, *spe, *psvol, *gammap;
+  double *bfil, *bder, *br, *brw, *dera, *q2ab, *abrw, *deru, *derv, *derh, *derus, *dervs;
+  double *g_gb, *g_vw, *g_cav, *g_hb; /* [natoms*3], internal order */
+  double *eatom;                      /* [7][natoms] */
+  double *ews;                        /* [nws] */
+  void *wpos, *wdpos;                 /* R[3*nws], R[36*nws] */
+  double *wsp;                        /* [nws] */
+  double *o_sp, *o_br, *o_sa, *o_gb, *o_gv, *o_gc, *o_gh;
+  int nbuckets;
+};
+
+enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m */, DC_C0 = DC_L0 + 8 /* candidates */ };
+#define DC_SIZE (DC_C0 + 8)
+
+/* record fields of a kept overlap */
+enum { F_A = 0, F_P, F_CX, F_CY, F_CZ, F_GVOL, F_GVOLP, F_FP, F_FPP, F_NUM };
+
+/* ------------------------------------------------------------------------ */
+/* math helpers                                                             */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ float m_exp(float x) { return expf(x); }
+__device__ __forceinline__ double m_exp(double x) { return exp(x); }
+__device__ __forceinline__ float m_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float m_rsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double m_rsqrt(double x) { return rsqrt(x); }
+
+template <typename R>
+__device__ __forceinline__ R px(const View &v, int g);
+template <>
+__device__ __forceinline__ float px<float>(const View &v, int g) { return v.pos[g].x; }
+template <>
+__device__ __forceinline__ double px<double>(const View &v, int g) { return v.pxd[g]; }
+template <typename R>
+__device__ __forceinline__ R py(const View &v, int g);
+template <>
+__device__ __forceinline__ float py<float>(const View &v, int g) { return v.pos[g].y; }
+template <>
+__device__ __forceinline__ double py<double>(const View &v, int g) { return v.pyd[g]; }
+template <typename R>
+__device__ __forceinline__ R pz(const View &v, int g);
+template <>
+__device__ __forceinline__ float pz<float>(const View &v, int g) { return v.pos[g].z; }
+template <>
+__device__ __forceinline__ double pz<double>(const View &v, int g) { return v.pzd[g]; }
+
+template <typename R>
+__device__ __forceinline__ const R *tables(const View &v);
+template <>
+__device__ __forceinline__ const float *tables<float>(const View &v) { return v.tab_f; }
+template <>
+__device__ __forceinline__ const double *tables<double>(const View &v) { return v.tab_d; }
+
+__device__ __forceinline__ void set_err(const View &v, int bit) { atomicOr(&v.dc[DC_ERR], bit); }
+
+/* quintic switch from 0 at xa to 1 at xb with first and second derivative
+   (agbnp3.c:1120-1145, agbnp3_cpu_simd_kernels.c:2487-2529) */
+template <typename R>
+__device__ __forceinline__ R poly_switch(R x, R xa, R xb, R &fp, R &fpp) {
+  if (x > xb) {
+    fp = fpp = R(0);
+    return R(1);
+  }
+  if (x < xa) {
+    fp = fpp = R(0);
+    return R(0);
+  }
+  R d = R(1) / (xb - xa), u = (x - xa) * d, u2 = u * u;
+  fp = d * R(30) * u2 * (R(1) - R(2) * u + u2);
+  fpp = d * d * R(60) * u * (R(1) - R(3) * u + R(2) * u2);
+  return u * u2 * (R(10) - R(15) * u + R(6) * u2);
+}
+
+/* product of two Gaussians a1 p1 (x1) and a2 p2 (x2): exponent, prefactor,
+   centre, raw overlap volume and the switched volume with its derivative
+   factors (agbnp3_cpu_simd_kernels.c:2418-2477) */
+template <typename R>
+struct Ov {
+  R a, p, cx, cy, cz, gvol, gvolp, fp, fpp;
+};
+
+template <typename R>
+__device__ __forceinline__ Ov<R> ogauss(R a1, R p1, R x1, R y1, R z1, R a2, R p2, R x2, R y2, R z2) {
+  Ov<R> o;
+  R dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
+  R d2 = dx * dx + dy * dy + dz * dz;
+  o.a = a1 + a2;
+  R inv = R(1) / o.a;
+  o.p = p1 * p2 * m_exp(-a1 * a2 * d2 * inv);
+  R u = R(C_PI) * inv;
+  o.gvol = o.p * u * m_sqrt(u);
+  o.cx = inv * (a1 * x1 + a2 * x2);
+  o.cy = inv * (a1 * y1 + a2 * y2);
+  o.cz = inv * (a1 * z1 + a2 * z2);
+  R sp, spp;
+  R s = poly_switch<R>(o.gvol, R(C_VOLA), R(C_VOLB), sp, spp);
+  o.gvolp = s * o.gvol;
+  o.fp = s + o.gvol * sp;
+  o.fpp = R(2) * sp + o.gvol * spp;
+  return o;
+}
+
+template <typename R>
+__device__ __forceinline__ bool kept(R gvolp) {
+  return gvolp > R(FLT_MIN);
+}
+
+/* Q4 of an atom (radius type td) descreened by a heavy atom of type ts and
+   radius Rs at distance d, and dQ4/dd; cubic-spline lookup at a = d/Rs
+   (agbnp3_utils.c:229-252, 297-377).  `ref_sign` keeps the reference's
+   sign of the second curvature term of the derivative (agbnp3_utils.c:
+   250-251). */
+template <typename R>
+__device__ __forceinline__ R q4(const R *tab, int ntypes, int td, int ts, R d, R Rs, R &dq, bool want_dq,
+                                bool ref_sign) {
+  const R h = R(C_AMAX / (AGB_NA - 1));
+  const R hinv = R((AGB_NA - 1) / C_AMAX);
+  R rinv = R(1) / Rs;
+  R xh = d * rinv * hinv;
+  int k = (int)xh;
+  if (k > AGB_NA - 2) {
+    dq = R(0);
+    return R(0);
+  }
+  const R *t = tab + ((size_t)(td * ntypes + ts) * AGB_NA + k) * 2;
+  R y0 = t[0], c0 = t[1], y1 = t[2], c1 = t[3];
+  R A = R(k + 1) - xh, B = xh - R(k);
+  R dp1 = h * R(1.0 / 6.0), dp2 = h * dp1;
+  R f = A * y0 + B * y1 + ((A * A * A - A) * c0 + (B * B * B - B) * c1) * dp2;
+  if (want_dq) {
+    R s2 = ref_sign ? R(1) : R(-1);
+    R fp = (y1 - y0) * hinv - ((R(3) * A * A - R(1)) * c0 + s2 * (R(3) * B * B - R(1)) * c1) * dp1;
+    dq = fp * rinv * rinv;
+  }
+  return f * rinv;
+}
+
+/* ------------------------------------------------------------------------ */
+/* prep: gather coordinates into internal order, reset accumulators         */
+/* ------------------------------------------------------------------------ */
+__global__ void k_prep(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int e = v.ext_of[g];
+    double x = v.x_ext[e], y = v.y_ext[e], z = v.z_ext[e], r = v.r[g];
+    f4 p;
+    p.x = (float)x;
+    p.y = (float)y;
+    p.z = (float)z;
+    p.w = (float)r;
+    v.pos[g] = p;
+    v.pxd[g] = x;
+    v.pyd[g] = y;
+    v.pzd[g] = z;
+    int I = v.inst_of[g];
+    bool heavy = g < v.inst_begin[I] + v.inst_nheavy[I];
+    v.volumep[g] = heavy ? v.vols[g] : 0.0;
+    v.surf[g] = heavy ? 4.0 * C_PI * r * r : 0.0;
+    v.dera[g] = v.deru[g] = v.derv[g] = v.derh[g] = 0.0;
+    for (int c = 0; c < 3; c++) {
+      v.g_gb[3 * g + c] = v.g_vw[3 * g + c] = v.g_cav[3 * g + c] = v.g_hb[3 * g + c] = 0.0;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* nblist: hashed cell grid over the heavy atoms of each instance           */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ int cell_hash(int cx, int cy, int cz, int mask) {
+  unsigned h = (unsigned)cx * 73856093u ^ (unsigned)cy * 19349663u ^ (unsigned)cz * 83492791u;
+  return (int)(h & (unsigned)mask);
+}
+
+__device__ __forceinline__ void cell_of(float x, float y, float z, float inv, int &cx, int &cy, int &cz) {
+  cx = (int)floorf(x * inv);
+  cy = (int)floorf(y * inv);
+  cz = (int)floorf(z * inv);
+}
+
+__global__ void k_cell_count(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int I = v.inst_of[g];
+    if (g >= v.inst_begin[I] + v.inst_nheavy[I]) continue;
+    float inv = 1.0f / v.inst_cell[I];
+    f4 p = v.pos[g];
+    int cx, cy, cz;
+    cell_of(p.x, p.y, p.z, inv, cx, cy, cz);
+    v.atom_cell[3 * g] = cx;
+    v.atom_cell[3 * g + 1] = cy;
+    v.atom_cell[3 * g + 2] = cz;
+    int b = v.bucket_begin[I] + cell_hash(cx, cy, cz, v.bucket_mask[I]);
+    v.atom_bucket[g] = b;
+    atomicAdd(&v.bucket_count[b], 1);
+  }
+}
+
+__global__ void k_cell_fill(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int I = v.inst_of[g];
+    if (g >= v.inst_begin[I] + v.inst_nheavy[I]) continue;
+    int b = v.atom_bucket[g];
+    /* slot order inside a bucket is arbitrary; every consumer sorts */
+    int s = atomicAdd(&v.bucket_cursor[b], 1);
+    v.cell_atoms[v.bucket_start[b] + s] = (int)g;
+  }
+}
+
+/* visits the heavy atoms of instance I in the 27 cells around cell c;
+   an atom is taken only from its own cell, so hash collisions never yield
+   duplicates.  fn(j) is called once per atom. */
+template <typename Fn>
+__device__ __forceinline__ void for_cell_neighbours(const View &v, int I, int cx, int cy, int cz, Fn fn) {
+  int mask = v.bucket_mask[I], base = v.bucket_begin[I];
+  for (int dz = -1; dz <= 1; dz++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        int ax = cx + dx, ay = cy + dy, az = cz + dz;
+        int b = base + cell_hash(ax, ay, az, mask);
+        int s0 = v.bucket_start[b], s1 = s0 + v.bucket_count[b];
+        for (int s = s0; s < s1; s++) {
+          int j = v.cell_atoms[s];
+          if (v.atom_cell[3 * j] != ax || v.atom_cell[3 * j + 1] != ay || v.atom_cell[3 * j + 2] != az) continue;
+          fn(j);
+        }
+      }
+}
+
+/* the reference's float membership test d^2 < (1.6 (ri + rj))^2, evaluated
+   without fused operations (agbnp3.c:4041-4049) */
+__device__ __forceinline__ bool near_test(const f4 &a, const f4 &b, float &d2) {
+  float dx = __fsub_rn(b.x, a.x), dy = __fsub_rn(b.y, a.y), dz = __fsub_rn(b.z, a.z);
+  d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+  float u = __fmul_rn(__fadd_rn(a.w, b.w), 1.6f);
+  return d2 < __fmul_rn(u, u);
+}
+
+__global__ void k_nl_count(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int I = v.inst_of[g];
+    int cnt = 0;
+    if (g < v.inst_begin[I] + v.inst_nheavy[I]) {
+      f4 a = v.pos[g];
+      for_cell_neighbours(v, I, v.atom_cell[3 * g], v.atom_cell[3 * g + 1], v.atom_cell[3 * g + 2], [&](int j) {
+        float d2;
+        if (j > g && near_test(a, v.pos[j], d2)) cnt++;
+      });
+    }
+    v.nl_count[g] = cnt;
+  }
+}
+
+__global__ void k_nl_emit(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int n = v.nl_count[g];
+    if (n == 0) continue;
+    int o = v.nl_off[g];
+    if (o + n > v.cap_nl) {
+      set_err(v, AGB_ERR_NL_CAP);
+      continue;
+    }
+    int I = v.inst_of[g];
+    f4 a = v.pos[g];
+    int m = 0;
+    int *lst = v.nl_list + o;
+    float *dd = v.nl_d2 + o;
+    for_cell_neighbours(v, I, v.atom_cell[3 * g], v.atom_cell[3 * g + 1], v.atom_cell[3 * g + 2], [&](int j) {
+      float d2;
+      if (j > g && near_test(a, v.pos[j], d2) && m < n) {
+        /* insertion into the (d^2, index)-sorted prefix
+           (agbnp3.c:3766-3792, 4062-4066) */
+        int k = m++;
+        while (k > 0 && (dd[k - 1] > d2 || (dd[k - 1] == d2 && lst[k - 1] > j))) {
+          dd[k] = dd[k - 1];
+          lst[k] = lst[k - 1];
+          k--;
+        }
+        dd[k] = d2;
+        lst[k] = j;
+      }
+    });
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* volumes: the overlap tree                                                */
+/* ------------------------------------------------------------------------ */
+template <typename R>
+__device__ __forceinline__ R atom_alpha(const View &v, int g) {
+  R r = (R)v.r[g];
+  return R(C_KFC) / (r * r);
+}
+
+template <typename R>
+__device__ __forceinline__ Ov<R> atom_pair(const View &v, int i, int j) {
+  return ogauss<R>(atom_alpha<R>(v, i), R(C_PFC), px<R>(v, i), py<R>(v, i), pz<R>(v, i), atom_alpha<R>(v, j),
+                   R(C_PFC), px<R>(v, j), py<R>(v, j), pz<R>(v, j));
+}
+
+template <typename R>
+__device__ __forceinline__ R rec_get(const View &v, int m, int q, int f) {
+  return ((const R *)v.rec[m])[(size_t)f * v.cap[m] + q];
+}
+
+template <typename R>
+__device__ __forceinline__ void rec_put(const View &v, int m, int q, const Ov<R> &o) {
+  R *b = (R *)v.rec[m];
+  size_t c = v.cap[m];
+  b[F_A * c + q] = o.a;
+  b[F_P * c + q] = o.p;
+  b[F_CX * c + q] = o.cx;
+  b[F_CY * c + q] = o.cy;
+  b[F_CZ * c + q] = o.cz;
+  b[F_GVOL * c + q] = o.gvol;
+  b[F_GVOLP * c + q] = o.gvolp;
+  b[F_FP * c + q] = o.fp;
+  b[F_FPP * c + q] = o.fpp;
+}
+
+/* self-volume and surface-area contributions of one kept overlap of order
+   m with parents par[] (agbnp3_cpu_simd_kernels.c:1322-1345) */
+template <typename R>
+__device__ __forceinline__ void add_volumes(const View &v, int m, const int *par, const Ov<R> &o) {
+  double coef = ((m & 1) ? 1.0 : -1.0) / m; /* (-1)^(m+1) / m */
+  R sgn = (m & 1) ? R(1) : R(-1);           /* m * coef */
+  R h3 = sgn * o.fp * R(3) / o.a, h4 = R(0.5) * sgn * o.fp;
+  for (int ii = 0; ii < m; ii++) {
+    int k = par[ii];
+    atomicAdd(&v.volumep[k], coef * (double)o.gvolp);
+    R u1 = atom_alpha<R>(v, k) * o.gvol, u2 = R(-2) * u1;
+    R v0 = u2 * (px<R>(v, k) - o.cx), v1 = u2 * (py<R>(v, k) - o.cy), v2 = u2 * (pz<R>(v, k) - o.cz);
+    R d2 = v0 * v0 + v1 * v1 + v2 * v2;
+    atomicAdd(&v.surf[k], (double)((h3 * u1 + h4 * d2 / u1) / (R)v.r[k]));
+  }
+}
+
+/* order 2: candidates are the near-list pairs of each heavy atom */
+template <typename R>
+__global__ void k_l2_count(View v) {
+  if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int n = v.nl_count[g], o = v.nl_off[g], cnt = 0;
+    if (n > 0 && o + n <= v.cap_nl)
+      for (int k = 0; k < n; k++) {
+        Ov<R> ov = atom_pair<R>(v, (int)g, v.nl_list[o + k]);
+        if (kept(ov.gvolp)) cnt++;
+      }
+    v.lv_cnt[2][g] = cnt;
+  }
+}
+
+template <typename R>
+__global__ void k_l2_emit(View v) {
+  if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int n = v.nl_count[g], o = v.nl_off[g];
+    if (n == 0 || o + n > v.cap_nl) continue;
+    int q = v.lv_off[2][g], qend = q + v.lv_cnt[2][g];
+    if (qend > v.cap[2]) {
+      set_err(v, AGB_ERR_TREE_CAP);
+      continue;
+    }
+    for (int k = 0; k < n; k++) {
+      int j = v.nl_list[o + k];
+      Ov<R> ov = atom_pair<R>(v, (int)g, j);
+      if (!kept(ov.gvolp)) continue;
+      int par[2] = {(int)g, j};
+      v.par[2][q] = par[0];
+      v.par[2][v.cap[2] + q] = par[1];
+      rec_put<R>(v, 2, q, ov);
+      v.gend[2][q] = qend;
+      add_volumes<R>(v, 2, par, ov);
+      q++;
+    }
+  }
+}
+
+/* order m >= 3: overlap a combines with the last atom of every later
+   overlap b of its group (same generating overlap one order down) */
+template <typename R>
+__global__ void k_lm_count(View v, int m) {
+  if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
+  int n = min(v.dc[DC_L0 + m - 1], v.cap[m - 1]);
+  int cm = v.cap[m - 1];
+  AGB_GRID_STRIDE(a, n) {
+    int ge = v.gend[m - 1][a], cnt = 0;
+    R aa = rec_get<R>(v, m - 1, a, F_A), ap = rec_get<R>(v, m - 1, a, F_P);
+    R ax = rec_get<R>(v, m - 1, a, F_CX), ay = rec_get<R>(v, m - 1, a, F_CY), az = rec_get<R>(v, m - 1, a, F_CZ);
+    for (int b = a + 1; b < ge; b++) {
+      int j = v.par[m - 1][(size_t)(m - 2) * cm + b];
+      Ov<R> ov = ogauss<R>(aa, ap, ax, ay, az, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j), pz<R>(v, j));
+      if (kept(ov.gvolp)) cnt++;
+    }
+    v.lv_cnt[m][a] = cnt;
+  }
+}
+
+template <typename R>
+__global__ void k_lm_emit(View v, int m) {
+  if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
+  int n = min(v.dc[DC_L0 + m - 1], v.cap[m - 1]);
+  int cm = v.cap[m - 1], cn = v.cap[m];
+  AGB_GRID_STRIDE(a, n) {
+    int q = v.lv_off[m][a], qend = q + v.lv_cnt[m][a];
+    if (q == qend) continue;
+    if (qend > cn) {
+      set_err(v, AGB_ERR_TREE_CAP);
+      continue;
+    }
+    int ge = v.gend[m - 1][a];
+    int par[AGB_MAX_ORDER];
+    for (int k = 0; k < m - 1; k++) par[k] = v.par[m - 1][(size_t)k * cm + a];
+    R aa = rec_get<R>(v, m - 1, a, F_A), ap = rec_get<R>(v, m - 1, a, F_P);
+    R ax = rec_get<R>(v, m - 1, a, F_CX), ay = rec_get<R>(v, m - 1, a, F_CY), az = rec_get<R>(v, m - 1, a, F_CZ);
+    for (int b = a + 1; b < ge; b++) {
+      int j = v.par[m - 1][(size_t)(m - 2) * cm + b];
+      Ov<R> ov = ogauss<R>(aa, ap, ax, ay, az, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j), pz<R>(v, j));
+      if (!kept(ov.gvolp)) continue;
+      par[m - 1] = j;
+      for (int k = 0; k < m; k++) v.par[m][(size_t)k * cn + q] = par[k];
+      rec_put<R>(v, m, q, ov);
+      v.gend[m][q] = qend;
+      add_volumes<R>(v, m, par, ov);
+      q++;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* scaling factors, filtered surface areas, cavity energy                   */
+/* ------------------------------------------------------------------------ */
+__global__ void k_scaling(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int I = v.inst_of[g];
+    size_t N = v.natoms;
+    if (g >= v.inst_begin[I] + v.inst_nheavy[I]) {
+      v.sp[g] = 1.0;
+      v.spe[g] = 0.0;
+      v.surf_f[g] = v.psvol[g] = v.gammap[g] = 0.0;
+      v.eatom[4 * N + g] = v.eatom[5 * N + g] = v.eatom[6 * N + g] = 0.0;
+      continue;
+    }
+    double A = v.surf[g], f, fp;
+    if (A < 0.0) { /* agbnp3.c:1104-1117 */
+      f = fp = 0.0;
+    } else {
+      double t = A / (64.0 + A * A);
+      f = A * t;
+      fp = 2.0 * t * (1.0 - f);
+    }
+    double sf = A * f, r = v.r[g], vol = v.vols[g];
+    v.surf_f[g] = sf;
+    v.gammap[g] = (v.igamma[g] + v.sgamma[g]) * (f + A * fp);
+    v.spe[g] = v.volumep[g] / vol;
+    double q = (r - C_RINC) / r;
+    double pr = r * (1.0 - q * q * q) / 3.0;
+    v.psvol[g] = (fp * A + f) * pr;
+    double vp = v.volumep[g] - sf * pr;
+    v.volumep[g] = vp;
+    v.sp[g] = vp / vol;
+    v.eatom[4 * N + g] = v.igamma[g] * sf;
+    v.eatom[5 * N + g] = v.sgamma[g] * sf;
+    v.eatom[6 * N + g] = vp;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* invb: descreening -> Born radii, vdW energy                              */
+/* ------------------------------------------------------------------------ */
+template <typename R>
+__global__ void k_descreen(View v) {
+  const R *tab = tables<R>(v);
+  size_t N = v.natoms;
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int I = v.inst_of[g];
+    int h0 = v.inst_begin[I], h1 = h0 + v.inst_nheavy[I];
+    R xg = px<R>(v, (int)g), yg = py<R>(v, (int)g), zg = pz<R>(v, (int)g);
+    int tg = v.rtype[g];
+    double acc = 0.0;
+    for (int h = h0; h < h1; h++) {
+      if (h == g) continue;
+      R dx = px<R>(v, h) - xg, dy = py<R>(v, h) - yg, dz = pz<R>(v, h) - zg;
+      R d = m_sqrt(dx * dx + dy * dy + dz * dz);
+      R dq;
+      R q = q4<R>(tab, v.ntypes, tg, v.rtype[h], d, (R)v.r[h], dq, false, false);
+      acc += (double)(q * (R)v.sp[h]);
+    }
+    /* inverse Born radius, its filter and the Born radius
+       (agbnp3_cpu_simd_kernels.c:605, agbnp3.c:1174-1188) */
+    double beta = 1.0 / (v.r[g] - C_RINC) - acc / (4.0 * C_PI);
+    double bf, bd;
+    if (beta < 0.0) {
+      bf = 0.02;
+      bd = 0.0;
+    } else {
+      bf = sqrt(0.02 * 0.02 + beta * beta);
+      bd = beta / bf;
+    }
+    double b = 1.0 / bf, t = b + C_RW;
+    v.bfil[g] = bf;
+    v.bder[g] = bd;
+    v.br[g] = b;
+    v.brw[g] = 3.0 * b * b / (t * t * t * t);
+    double a3 = 1.0 / (t * t * t);
+    v.eatom[2 * N + g] = v.ialpha[g] * a3;
+    v.eatom[3 * N + g] = v.salpha[g] * a3;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* agb: GB pair energy, gradient at constant Born radii, A_i                */
+/* ------------------------------------------------------------------------ */
+template <typename R>
+__global__ void k_gbpair(View v) {
+  size_t N = v.natoms;
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int I = v.inst_of[g];
+    int j0 = v.inst_begin[I], j1 = v.inst_begin[I + 1];
+    double df = v.inst_df[I];
+    R xi = px<R>(v, (int)g), yi = py<R>(v, (int)g), zi = pz<R>(v, (int)g);
+    R qi = (R)v.charge[g], bi = (R)v.br[g];
+    R qf = R(2.0 * df);
+    double e = 0.0, at = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int j = j0; j < j1; j++) {
+      R dx = px<R>(v, j) - xi, dy = py<R>(v, j) - yi, dz = pz<R>(v, j) - zi;
+      R d2 = dx * dx + dy * dy + dz * dz;
+      if (!(d2 > R(0))) continue; /* the pair itself and coincident atoms */
+      R qq = qi * (R)v.charge[j];
+      R bb = bi * (R)v.br[j];
+      R et = m_exp(R(-0.25) * d2 / bb);
+      R f = m_rsqrt(d2 + bb * et);
+      R f3 = f * f * f;
+      R w = qf * qq;
+      e += (double)(w * f);
+      R mw = -w * (R(1) - R(0.25) * et) * f3;
+      gx -= (double)(mw * dx);
+      gy -= (double)(mw * dy);
+      gz -= (double)(mw * dz);
+      at += (double)(qq * (bb + R(0.25) * d2) * et * f3);
+    }
+    double q = v.charge[g], b = v.br[g];
+    v.g_gb[3 * g] += gx;
+    v.g_gb[3 * g + 1] += gy;
+    v.g_gb[3 * g + 2] += gz;
+    v.dera[g] = at;
+    v.eatom[g] = C_TOKCAL * df * q * q / b;
+    v.eatom[N + g] = C_TOKCAL * 0.5 * e;
+    /* agbnp3_cpu_simd_kernels.c:444-449 */
+    v.q2ab[g] = (q * q + at * b) * v.bder[g];
+    v.abrw[g] = (v.ialpha[g] + v.salpha[g]) * v.brw[g] * v.bder[g];
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* gbders: gradient through the Born radii at constant self volumes, U, V   */
+/* ------------------------------------------------------------------------ */
+template <typename R>
+__global__ void k_gbders(View v) {
+  const R *tab = tables<R>(v);
+  const bool rs = v.compat != 0;
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int I = v.inst_of[g];
+    int h0 = v.inst_begin[I], hh = h0 + v.inst_nheavy[I], j1 = v.inst_begin[I + 1];
+    bool heavy = g < hh;
+    double df = v.inst_df[I];
+    R xa = px<R>(v, (int)g), ya = py<R>(v, (int)g), za = pz<R>(v, (int)g);
+    int ta = v.rtype[g];
+    R ra = (R)v.r[g], spa = (R)v.sp[g];
+    R q2a = (R)v.q2ab[g], aba = (R)v.abrw[g];
+    double u = 0.0, w = 0.0, gbx = 0, gby = 0, gbz = 0, gvx = 0, gvy = 0, gvz = 0;
+    int jend = heavy ? j1 : hh; /* hydrogens are only descreened */
+    for (int b = h0; b < jend; b++) {
+      if (b == g) continue;
+      R dx = px<R>(v, b) - xa, dy = py<R>(v, b) - ya, dz = pz<R>(v, b) - za;
+      R d = m_sqrt(dx * dx + dy * dy + dz * dz);
+      if (!(d > R(0))) continue;
+      R ht = R(0), ut = R(0);
+      if (heavy) { /* b descreened by a */
+        R dq;
+        R q = q4<R>(tab, v.ntypes, v.rtype[b], ta, d, ra, dq, true, rs);
+        R q2b = (R)v.q2ab[b], abb = (R)v.abrw[b];
+        u += (double)(q2b * q);
+        w += (double)(abb * q);
+        ht += q2b * dq * spa;
+        ut += abb * dq * spa;
+      }
+      if (b < hh) { /* a descreened by b */
+        R dq;
+        q4<R>(tab, v.ntypes, ta, v.rtype[b], d, (R)v.r[b], dq, true, rs);
+        R spb = (R)v.sp[b];
+        ht += q2a * dq * spb;
+        ut += aba * dq * spb;
+      }
+      R id = R(1) / d;
+      double hs = (double)(ht * id), us = (double)(ut * id);
+      gbx += hs * (double)dx;
+      gby += hs * (double)dy;
+      gbz += hs * (double)dz;
+      gvx += us * (double)dx;
+      gvy += us * (double)dy;
+      gvz += us * (double)dz;
+    }
+    const double f4p = 1.0 / (4.0 * C_PI);
+    v.g_gb[3 * g] += f4p * df * gbx;
+    v.g_gb[3 * g + 1] += f4p * df * gby;
+    v.g_gb[3 * g + 2] += f4p * df * gbz;
+    v.g_vw[3 * g] += f4p * gvx;
+    v.g_vw[3 * g + 1] += f4p * gvy;
+    v.g_vw[3 * g + 2] += f4p * gvz;
+    if (heavy) { /* agbnp3_cpu_simd_kernels.c:861-874 */
+      double vol = v.vols[g];
+      double du = u / vol, dv = w / vol;
+      v.deru[g] = du;
+      v.derv[g] = dv;
+      v.dervs[g] = f4p * v.psvol[g] * dv;
+      v.derus[g] = df * f4p * v.psvol[g] * du;
+    } else {
+      v.deru[g] = v.derv[g] = v.dervs[g] = v.derus[g] = 0.0;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* ws: water-site geometry and Jacobians                                    */
+/* ------------------------------------------------------------------------ */
+template <typename R>
+struct V3 {
+  R x, y, z;
+};
+template <typename R>
+__device__ __forceinline__ V3<R> vsub(V3<R> a, V3<R> b) {
+  return {a.x - b.x, a.y - b.y, a.z - b.z};
+}
+template <typename R>
+__device__ __forceinline__ R vnorm(V3<R> a) {
+  return m_sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+}
+template <typename R>
+__device__ __forceinline__ V3<R> vscale(V3<R> a, R s) {
+  return {a.x * s, a.y * s, a.z * s};
+}
+template <typename R>
+__device__ __forceinline__ V3<R> vcross(V3<R> a, V3<R> b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <typename R>
+__device__ __forceinline__ R vc(V3<R> a, int i) {
+  return i == 0 ? a.x : (i == 1 ? a.y : a.z);
+}
+template <typename R>
+__device__ __forceinline__ V3<R> atom_v(const View &v, int g) {
+  return {px<R>(v, g), py<R>(v, g), pz<R>(v, g)};
+}
+
+/* (I - u u^T) / L : derivative of the unit vector of a vector of length L */
+template <typename R>
+__device__ __forceinline__ void unit_der(V3<R> u, R invL, R D[3][3]) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) D[i][j] = invL * ((i == j ? R(1) : R(0)) - vc(u, i) * vc(u, j));
+}
+/* C = A B */
+template <typename R>
+__device__ __forceinline__ void mmul(const R A[3][3], const R B[3][3], R C[3][3]) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) C[i][j] = A[i][0] * B[0][j] + A[i][1] * B[1][j] + A[i][2] * B[2][j];
+}
+/* d(a x b)/db (rows: components of a x b) */
+template <typename R>
+__device__ __forceinline__ void cross_der_b(V3<R> a, R D[3][3]) {
+  D[0][0] = 0; D[0][1] = -a.z; D[0][2] = a.y;
+  D[1][0] = a.z; D[1][1] = 0; D[1][2] = -a.x;
+  D[2][0] = -a.y; D[2][1] = a.x; D[2][2] = 0;
+}
+/* d(a x b)/da */
+template <typename R>
+__device__ __forceinline__ void cross_der_a(V3<R> b, R D[3][3]) {
+  D[0][0] = 0; D[0][1] = b.z; D[0][2] = -b.y;
+  D[1][0] = -b.z; D[1][1] = 0; D[1][2] = b.x;
+  D[2][0] = b.y; D[2][1] = -b.x; D[2][2] = 0;
+}
+
+template <typename R>
+__global__ void k_ws_geom(View v) {
+  R *wpos = (R *)v.wpos, *wd = (R *)v.wdpos;
+  const R L = R(C_HBLEN);
+  AGB_GRID_STRIDE(w, v.nws) {
+    const int *P = v.ws_parent + 4 * w;
+    int kind = v.ws_kind[w];
+    R D[4][3][3];
+    for (int p = 0; p < 4; p++)
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) D[p][i][j] = R(0);
+    V3<R> pos;
+    V3<R> A = atom_v<R>(v, P[0]);
+    if (kind == WK_POLARH) { /* parents: hydrogen, heavy atom */
+      V3<R> Xd = atom_v<R>(v, P[1]);
+      V3<R> b = vsub(A, Xd);
+      R len = vnorm(b), s = L / len;
+      V3<R> u = vscale(b, R(1) / len);
+      pos = {Xd.x + s * b.x, Xd.y + s * b.y, Xd.z + s * b.z};
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+          R pr = (i == j ? R(1) : R(0)) - vc(u, i) * vc(u, j);
+          D[0][i][j] = s * pr;
+          D[1][i][j] = (i == j ? R(1) : R(0)) - s * pr;
+        }
+    } else if (kind == WK_TRIG1_A || kind == WK_TRIG1_B || kind == WK_TET1) {
+      /* anti-parallel to R-Rk, from the acceptor: parents A, R, (R1, R2 | Rk) */
+      int pk = kind == WK_TRIG1_A ? 2 : (kind == WK_TRIG1_B ? 3 : 2);
+      V3<R> Rr = atom_v<R>(v, P[1]), Rk = atom_v<R>(v, P[pk]);
+      V3<R> b = vsub(Rk, Rr);
+      R len = vnorm(b);
+      V3<R> u = vscale(b, R(1) / len);
+      pos = {A.x - L * u.x, A.y - L * u.y, A.z - L * u.z};
+      for (int i = 0; i < 3; i++) {
+        D[0][i][i] = R(1);
+        for (int j = 0; j < 3; j++) {
+          R gg = (L / len) * ((i == j ? R(1) : R(0)) - vc(u, i) * vc(u, j));
+          D[1][i][j] = gg;
+          D[pk][i][j] = -gg;
+        }
+      }
+    } else if (kind == WK_TRIGS_A || kind == WK_TRIGS_B) {
+      /* 60 degrees off the R->A axis towards +-(R1-R) x (A-R); parents A, R, R1, R2 */
+      const R cth = R(0.5), sth = R(0.866025);
+      R sg = kind == WK_TRIGS_A ? R(1) : R(-1);
+      V3<R> Rr = atom_v<R>(v, P[1]), R1 = atom_v<R>(v, P[2]);
+      V3<R> e0 = vsub(A, Rr), e1 = vsub(R1, Rr);
+      R l0 = vnorm(e0);
+      V3<R> uin = vscale(e0, R(1) / l0);
+      V3<R> n = vcross(e1, e0);
+      R ln = vnorm(n);
+      V3<R> uout = vscale(n, R(1) / ln);
+      pos = {A.x + L * (cth * uin.x + sg * sth * uout.x), A.y + L * (cth * uin.y + sg * sth * uout.y),
+             A.z + L * (cth * uin.z + sg * sth * uout.z)};
+      R Din[3][3], Dout[3][3], Ce0[3][3], Ce1[3][3], G0[3][3], G1[3][3];
+      unit_der(uin, R(1) / l0, Din);
+      unit_der(uout, R(1) / ln, Dout);
+      cross_der_b(e1, Ce0); /* d(e1 x e0)/de0 */
+      cross_der_a(e0, Ce1); /* d(e1 x e0)/de1 */
+      mmul(Dout, Ce0, G0);
+      mmul(Dout, Ce1, G1);
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+          R gin = L * cth * Din[i][j], g0 = sg * L * sth * G0[i][j], g1 = sg * L * sth * G1[i][j];
+          D[0][i][j] = gin + g0 + (i == j ? R(1) : R(0));
+          D[1][i][j] = -gin - g0 - g1;
+          D[2][i][j] = g1;
+        }
+    } else if (kind == WK_OOP_A || kind == WK_OOP_B) {
+      /* along +-normal of the R1 R2 R3 plane at 2.7 A; parents A, R1, R2, R3 */
+      const R dist = R((float)(C_HBLEN + 0.2));
+      R sg = kind == WK_OOP_A ? R(1) : R(-1);
+      V3<R> R1 = atom_v<R>(v, P[1]), R2 = atom_v<R>(v, P[2]), R3 = atom_v<R>(v, P[3]);
+      V3<R> v1 = vsub(R2, R1), v2 = vsub(R3, R1);
+      V3<R> n = vcross(v2, v1);
+      R ln = vnorm(n);
+      V3<R> nu = vscale(n, R(1) / ln);
+      pos = {A.x + sg * dist * nu.x, A.y + sg * dist * nu.y, A.z + sg * dist * nu.z};
+      R Pm[3][3], C1[3][3], C2[3][3], G1[3][3], G2[3][3];
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) Pm[i][j] = (i == j ? R(1) : R(0)) - vc(nu, i) * vc(nu, j);
+      cross_der_b(v2, C1); /* d(v2 x v1)/dv1 */
+      cross_der_a(v1, C2); /* d(v2 x v1)/dv2 */
+      mmul(Pm, C1, G1);
+      mmul(Pm, C2, G2);
+      R sc = sg * dist / ln;
+      for (int i = 0; i < 3; i++) {
+        D[0][i][i] = R(1);
+        for (int j = 0; j < 3; j++) {
+          D[2][i][j] = sc * G1[i][j];
+          D[3][i][j] = sc * G2[i][j];
+          D[1][i][j] = -(D[2][i][j] + D[3][i][j]);
+        }
+      }
+    } else if (kind == WK_BIS2 || kind == WK_BIS3) {
+      /* opposite the sum of the bond unit vectors; parents A, R1, R2 (, R3) */
+      int nb = kind == WK_BIS2 ? 2 : 3;
+      V3<R> u[3];
+      R inv[3];
+      V3<R> s = {R(0), R(0), R(0)};
+      for (int q = 0; q < nb; q++) {
+        V3<R> b = vsub(atom_v<R>(v, P[q + 1]), A);
+        R len = vnorm(b);
+        inv[q] = R(1) / len;
+        u[q] = vscale(b, inv[q]);
+        s.x += u[q].x;
+        s.y += u[q].y;
+        s.z += u[q].z;
+      }
+      R ls = vnorm(s);
+      V3<R> us = vscale(s, R(1) / ls);
+      pos = {A.x - L * us.x, A.y - L * us.y, A.z - L * us.z};
+      R Ds[3][3];
+      unit_der(us, R(1) / ls, Ds);
+      for (int i = 0; i < 3; i++) D[0][i][i] = R(1);
+      for (int q = 0; q < nb; q++) {
+        R Dq[3][3], G[3][3];
+        unit_der(u[q], inv[q], Dq);
+        mmul(Ds, Dq, G);
+        for (int i = 0; i < 3; i++)
+          for (int j = 0; j < 3; j++) {
+            D[q + 1][i][j] = -L * G[i][j];
+            D[0][i][j] += L * G[i][j];
+          }
+      }
+    } else { /* WK_TET2_A / WK_TET2_B: parents A, R1, R2 */
+      const R cth = R(-0.577350269), sth = R(0.816496581);
+      R sg = kind == WK_TET2_A ? R(1) : R(-1);
+      V3<R> r1 = vsub(atom_v<R>(v, P[1]), A), r2 = vsub(atom_v<R>(v, P[2]), A);
+      R l1 = vnorm(r1), l2 = vnorm(r2);
+      V3<R> u1 = vscale(r1, R(1) / l1), u2 = vscale(r2, R(1) / l2);
+      V3<R> s = {u1.x + u2.x, u1.y + u2.y, u1.z + u2.z};
+      R ls = vnorm(s);
+      V3<R> uin = vscale(s, R(1) / ls);
+      V3<R> n = vcross(r2, r1);
+      R ln = vnorm(n);
+      V3<R> uout = vscale(n, R(1) / ln);
+      pos = {A.x + L * (cth * uin.x + sg * sth * uout.x), A.y + L * (cth * uin.y + sg * sth * uout.y),
+             A.z + L * (cth * uin.z + sg * sth * uout.z)};
+      R Ds[3][3], D1[3][3], D2[3][3], Gi1[3][3], Gi2[3][3], Do[3][3], C1[3][3], C2[3][3], Go1[3][3], Go2[3][3];
+      unit_der(uin, R(1) / ls, Ds);
+      unit_der(u1, R(1) / l1, D1);
+      unit_der(u2, R(1) / l2, D2);
+      mmul(Ds, D1, Gi1);
+      mmul(Ds, D2, Gi2);
+      unit_der(uout, R(1) / ln, Do);
+      cross_der_b(r2, C1); /* d(r2 x r1)/dr1 */
+      cross_der_a(r1, C2); /* d(r2 x r1)/dr2 */
+      mmul(Do, C1, Go1);
+      mmul(Do, C2, Go2);
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+          R a1 = L * cth * Gi1[i][j] + sg * L * sth * Go1[i][j];
+          R a2 = L * cth * Gi2[i][j] + sg * L * sth * Go2[i][j];
+          D[1][i][j] = a1;
+          D[2][i][j] = a2;
+          D[0][i][j] = -(a1 + a2) + (i == j ? R(1) : R(0));
+        }
+    }
+    wpos[3 * w] = pos.x;
+    wpos[3 * w + 1] = pos.y;
+    wpos[3 * w + 2] = pos.z;
+    for (int p = 0; p < 4; p++)
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) wd[(size_t)w * 36 + p * 9 + i * 3 + j] = D[p][i][j];
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* ws: free volumes, HB energy and gradient                                 */
+/* ------------------------------------------------------------------------ */
+template <typename R>
+__global__ void k_ws_free(View v) {
+  const R *wpos = (const R *)v.wpos, *wd = (const R *)v.wdpos;
+  const R vw = R(4.0 / 3.0 * C_PI * C_HBRAD * C_HBRAD * C_HBRAD);
+  const R aw = R(C_KFC / (C_HBRAD * C_HBRAD));
+  AGB_GRID_STRIDE(w, v.nws) {
+    int I = v.ws_inst[w];
+    V3<R> p = {wpos[3 * w], wpos[3 * w + 1], wpos[3 * w + 2]};
+    int cand[WS_MAXC];
+    int nc = 0;
+    bool over = false;
+    float inv = 1.0f / v.inst_cell[I];
+    int cx, cy, cz;
+    cell_of((float)p.x, (float)p.y, (float)p.z, inv, cx, cy, cz);
+    /* heavy atoms with d^2 < (1.6 (r + 1.4))^2, in index order
+       (agbnp3_cpu_simd_kernels.c:2786-2811) */
+    for_cell_neighbours(v, I, cx, cy, cz, [&](int h) {
+      R dx = px<R>(v, h) - p.x, dy = py<R>(v, h) - p.y, dz = pz<R>(v, h) - p.z;
+      R u = ((R)v.r[h] + R(C_HBRAD)) * R(1.6);
+      if (dx * dx + dy * dy + dz * dz < u * u) {
+        if (nc == WS_MAXC) {
+          over = true;
+          return;
+        }
+        int k = nc++;
+        while (k > 0 && cand[k - 1] > h) {
+          cand[k] = cand[k - 1];
+          k--;
+        }
+        cand[k] = h;
+      }
+    });
+    if (over) set_err(v, AGB_ERR_WS_CAP);
+    /* free volume: subtract spe-weighted overlaps in index order until the
+       free volume drops to 60% (agbnp3_cpu_simd_kernels.c:2831-2895) */
+    double fv = (double)vw, cut = C_HBSWA0 * (double)vw;
+    int prev = v.ws_prev[w];
+    int np = 0;
+    for (int c = 0; c < nc; c++) {
+      if (!(fv > cut)) break;
+      int h = cand[c];
+      Ov<R> o = ogauss<R>(aw, R(C_PFC), p.x, p.y, p.z, atom_alpha<R>(v, h), R(C_PFC), px<R>(v, h), py<R>(v, h),
+                          pz<R>(v, h));
+      if (!(o.gvolp > R(0))) continue;
+      double s_used = v.compat ? (prev >= 0 ? v.spe[prev] : 0.0) : v.spe[h];
+      fv -= s_used * (double)o.gvolp;
+      prev = h;
+      cand[np++] = h;
+    }
+    double spw = fv / (double)vw, fp, fpp;
+    double sw = poly_switch<double>(spw, C_HBSWA, C_HBSWB, fp, fpp);
+    double khb = v.ws_khb[w];
+    double dhw = khb * fp / (double)vw;
+    v.ews[w] = khb * sw;
+    v.wsp[w] = spw;
+    /* derivatives (agbnp3_cpu_simd_kernels.c:2904-2933) */
+    double jw[3] = {0, 0, 0};
+    for (int c = 0; c < np; c++) {
+      int h = cand[c];
+      R ah = atom_alpha<R>(v, h);
+      Ov<R> o = ogauss<R>(aw, R(C_PFC), p.x, p.y, p.z, ah, R(C_PFC), px<R>(v, h), py<R>(v, h), pz<R>(v, h));
+      double sh = v.spe[h];
+      double fi = -2.0 * (double)(ah * o.gvol * o.fp), fw = -2.0 * (double)(aw * o.gvol * o.fp);
+      double uu = -sh * dhw;
+      atomicAdd(&v.g_hb[3 * h], uu * fi * (double)(px<R>(v, h) - o.cx));
+      atomicAdd(&v.g_hb[3 * h + 1], uu * fi * (double)(py<R>(v, h) - o.cy));
+      atomicAdd(&v.g_hb[3 * h + 2], uu * fi * (double)(pz<R>(v, h) - o.cz));
+      atomicAdd(&v.derh[h], dhw / v.vols[h] * (double)o.gvolp);
+      jw[0] += uu * fw * (double)(p.x - o.cx);
+      jw[1] += uu * fw * (double)(p.y - o.cy);
+      jw[2] += uu * fw * (double)(p.z - o.cz);
+    }
+    int npar = v.ws_nparent[w];
+    for (int q = 0; q < npar; q++) {
+      int a = v.ws_parent[4 * w + q];
+      for (int j = 0; j < 3; j++) {
+        double t = 0.0;
+        for (int k = 0; k < 3; k++) t += jw[k] * (double)wd[(size_t)w * 36 + q * 9 + k * 3 + j];
+        atomicAdd(&v.g_hb[3 * a + j], t);
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* treeders: derivatives through the self volumes and surface areas         */
+/* ------------------------------------------------------------------------ */
+template <typename R>
+__global__ void k_tree_ders(View v, int m) {
+  if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
+  int n = min(v.dc[DC_L0 + m], v.cap[m]);
+  int cm = v.cap[m];
+  const double f4p = 1.0 / (4.0 * C_PI);
+  double coef = ((m & 1) ? 1.0 : -1.0) / m;
+  double sgn = (m & 1) ? 1.0 : -1.0;
+  AGB_GRID_STRIDE(q, n) {
+    int par[AGB_MAX_ORDER];
+    for (int k = 0; k < m; k++) par[k] = v.par[m][(size_t)k * cm + q];
+    R cx = rec_get<R>(v, m, q, F_CX), cy = rec_get<R>(v, m, q, F_CY), cz = rec_get<R>(v, m, q, F_CZ);
+    R gvol = rec_get<R>(v, m, q, F_GVOL), fp = rec_get<R>(v, m, q, F_FP), fpp = rec_get<R>(v, m, q, F_FPP);
+    R inva = R(1) / rec_get<R>(v, m, q, F_A);
+    int I = v.inst_of[par[0]];
+    double df = v.inst_df[I];
+    double su = 0, sv = 0, sh = 0;
+    for (int k = 0; k < m; k++) {
+      su += v.deru[par[k]];
+      sv += v.derv[par[k]];
+      sh += v.derh[par[k]];
+    }
+    su *= -df * f4p * coef;
+    sv *= -f4p * coef;
+    sh *= -coef;
+    R gdr[AGB_MAX_ORDER][3], gdR[AGB_MAX_ORDER], ga[AGB_MAX_ORDER], gr[AGB_MAX_ORDER];
+    double acc[AGB_MAX_ORDER][4][3]; /* gb, vw, hb, cav per parent */
+    for (int ii = 0; ii < m; ii++) {
+      int k = par[ii];
+      ga[ii] = atom_alpha<R>(v, k);
+      gr[ii] = (R)v.r[k];
+      R u1 = ga[ii] * gvol;
+      R xk[3] = {px<R>(v, k) - cx, py<R>(v, k) - cy, pz<R>(v, k) - cz};
+      R d2 = R(0);
+      for (int c = 0; c < 3; c++) {
+        gdr[ii][c] = R(-2) * u1 * xk[c];
+        d2 += gdr[ii][c] * gdr[ii][c];
+        double ur = (double)(gdr[ii][c] * fp); /* -2 u1 fp (x - c) */
+        acc[ii][0][c] = su * ur;
+        acc[ii][1][c] = sv * ur;
+        acc[ii][2][c] = sh * ur;
+        acc[ii][3][c] = 0.0;
+      }
+      gdR[ii] = (R(3) * inva * u1 + R(0.5) * d2 / u1) / gr[ii];
+    }
+    R h3 = fpp + fp / gvol;
+    for (int ii = 0; ii < m; ii++) { /* diagonal terms */
+      int k = par[ii];
+      R u1 = R(-2) * fp * (R(1) - ga[ii] * inva) / gr[ii] + h3 * gdR[ii];
+      double wc = sgn * v.gammap[k], wv = sgn * v.dervs[k], wb = sgn * v.derus[k];
+      for (int c = 0; c < 3; c++) {
+        double ur = (double)(u1 * gdr[ii][c]);
+        acc[ii][3][c] += wc * ur;
+        acc[ii][1][c] += wv * ur;
+        acc[ii][0][c] += wb * ur;
+      }
+    }
+    R h4 = R(2) * fp * inva;
+    for (int ii = 0; ii < m; ii++) /* off-diagonal terms */
+      for (int jj = 0; jj < m; jj++) {
+        if (jj == ii) continue;
+        int l = par[jj];
+        R u1 = h4 * ga[ii] / gr[jj], u2 = h3 * gdR[jj];
+        double wc = sgn * v.gammap[l], wv = sgn * v.dervs[l], wb = sgn * v.derus[l];
+        for (int c = 0; c < 3; c++) {
+          double ur = (double)(u1 * gdr[jj][c] + u2 * gdr[ii][c]);
+          acc[ii][3][c] += wc * ur;
+          acc[ii][1][c] += wv * ur;
+          acc[ii][0][c] += wb * ur;
+        }
+      }
+    for (int ii = 0; ii < m; ii++) {
+      int k = par[ii];
+      for (int c = 0; c < 3; c++) {
+        atomicAdd(&v.g_gb[3 * k + c], acc[ii][0][c]);
+        atomicAdd(&v.g_vw[3 * k + c], acc[ii][1][c]);
+        atomicAdd(&v.g_hb[3 * k + c], acc[ii][2][c]);
+        atomicAdd(&v.g_cav[3 * k + c], acc[ii][3][c]);
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* final: outputs in caller order (agbnp3.c:1761-1786, 537-563)             */
+/* ------------------------------------------------------------------------ */
+__global__ void k_final(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int e = v.ext_of[g];
+    int I = v.inst_of[g];
+    bool heavy = g < v.inst_begin[I] + v.inst_nheavy[I];
+    v.o_sp[e] = heavy ? v.sp[g] : 1.0;
+    v.o_br[e] = v.br[g];
+    v.o_sa[e] = heavy ? v.surf_f[g] : 0.0;
+    for (int c = 0; c < 3; c++) {
+      v.o_gb[3 * e + c] = C_TOKCAL * v.g_gb[3 * g + c];
+      v.o_gv[3 * e + c] = v.g_vw[3 * g + c];
+      v.o_gc[3 * e + c] = v.g_cav[3 * g + c];
+      v.o_gh[3 * e + c] = v.g_hb[3 * g + c];
+    }
+  }
+}
+
+/* per-instance energies from the segment sums: rows of esum are
+   eself, epair, evdw, ecorr_vdw, ecav, ecorr_cav, mol_volume (per instance)
+   and ehb (per instance) */
+__global__ void k_energies(const double *esum, const double *ehb, int ninst, double *out, int *dc) {
+  AGB_GRID_STRIDE(I, ninst) {
+    double e[7];
+    e[0] = esum[I] + esum[ninst + I];
+    e[1] = esum[2 * ninst + I];
+    e[2] = esum[3 * ninst + I];
+    e[3] = esum[4 * ninst + I];
+    e[4] = esum[5 * ninst + I];
+    e[5] = ehb[I];
+    e[6] = esum[6 * ninst + I];
+    for (int k = 0; k < 7; k++) {
+      out[7 * I + k] = e[k];
+      if (!isfinite(e[k])) atomicOr(&dc[DC_ERR], AGB_ERR_NONFINITE);
+    }
+  }
+}
+
+/* ======================================================================== */
+/* host side                                                                */
+/* ======================================================================== */
+static char g_err[512];
+#define FAIL(...)                                  \
+  do {                                             \
+    snprintf(g_err, sizeof(g_err), __VA_ARGS__);   \
+    return -1;                                     \
+  } while (0)
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) FAIL("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+extern "C" const char *agb_dev_last_error(void) { return g_err; }
+
+static const char *stage_names[AGB_NSTAGE] = {"prep",  "nblist", "volumes", "scaling", "invb",  "agb",
+                                              "gbders", "ws",     "treeders", "final",  "reduce", "spare"};
+
+extern "C" const char *agb_dev_stage_name(int i) { return (i >= 0 && i < AGB_NSTAGE) ? stage_names[i] : ""; }
+
+struct agb_dev {
+  int device;
+  cudaStream_t st;
+  int ninst, natoms, nws, ntypes, precision, compat;
+  int *h_inst_begin, *h_ws_begin;
+  View v;
+  /* owned allocations */
+  void *allocs[128];
+  int nallocs;
+  /* tree capacity (owned separately, regrown on overflow) */
+  int cap_nl, cap[AGB_MAX_ORDER + 1];
+  int *scan_scratch;
+  int scan_cap;
+  double *esum, *ehb_inst, *o_energy;
+  int *nl_scan_len;
+  cudaGraphExec_t gexec;
+  int graph_ok;
+  int timing;
+  cudaEvent_t ev[AGB_NSTAGE + 1];
+  double stage_ms[AGB_NSTAGE];
+  long long nlaunch;
+  long long last_stats[16];
+};
+
+static int dev_alloc(agb_dev *s, void **p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) FAIL("cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  if (s->nallocs >= (int)(sizeof(s->allocs) / sizeof(s->allocs[0]))) FAIL("too many device allocations");
+  s->allocs[s->nallocs++] = *p;
+  return 0;
+}
+
+#define DALLOC(ptr, n, T)                                                        \
+  do {                                                                           \
+    void *p_;                                                                    \
+    if (dev_alloc(s, &p_, (size_t)(n) * sizeof(T)) != 0) return -1;              \
+    (ptr) = (T *)p_;                                                             \
+  } while (0)
+
+static int upload(void *dst, const void *src, size_t bytes) {
+  if (bytes == 0) return 0;
+  CK(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+static int tree_free(agb_dev *s) {
+  for (int m = 2; m <= AGB_MAX_ORDER; m++) {
+    if (s->v.par[m]) cudaFree(s->v.par[m]);
+    if (s->v.rec[m]) cudaFree(s->v.rec[m]);
+    if (s->v.gend[m]) cudaFree(s->v.gend[m]);
+    s->v.par[m] = NULL;
+    s->v.rec[m] = NULL;
+    s->v.gend[m] = NULL;
+  }
+  for (int m = 3; m <= AGB_MAX_ORDER; m++) {
+    if (s->v.lv_cnt[m]) cudaFree(s->v.lv_cnt[m]);
+    if (s->v.lv_off[m]) cudaFree(s->v.lv_off[m]);
+    s->v.lv_cnt[m] = s->v.lv_off[m] = NULL;
+  }
+  if (s->v.nl_list) cudaFree(s->v.nl_list);
+  if (s->v.nl_d2) cudaFree(s->v.nl_d2);
+  if (s->scan_scratch) cudaFree(s->scan_scratch);
+  s->v.nl_list = NULL;
+  s->v.nl_d2 = NULL;
+  s->scan_scratch = NULL;
+  return 0;
+}
+
+static int tree_alloc(agb_dev *s) {
+  size_t rsz = sizeof(double); /* records sized for the wider type */
+  CK(cudaMalloc((void **)&s->v.nl_list, sizeof(int) * (size_t)s->cap_nl));
+  CK(cudaMalloc((void **)&s->v.nl_d2, sizeof(float) * (size_t)s->cap_nl));
+  int maxcap = s->natoms;
+  for (int m = 2; m <= AGB_MAX_ORDER; m++) {
+    CK(cudaMalloc((void **)&s->v.par[m], sizeof(int) * (size_t)m * s->cap[m]));
+    CK(cudaMalloc(&s->v.rec[m], rsz * F_NUM * (size_t)s->cap[m]));
+    CK(cudaMalloc((void **)&s->v.gend[m], sizeof(int) * (size_t)s->cap[m]));
+    if (s->cap[m] > maxcap) maxcap = s->cap[m];
+    s->v.cap[m] = s->cap[m];
+  }
+  for (int m = 3; m <= AGB_MAX_ORDER; m++) {
+    /* one count / offset per generating overlap of order m-1 */
+    CK(cudaMalloc((void **)&s->v.lv_cnt[m], sizeof(int) * (size_t)s->cap[m - 1]));
+    CK(cudaMalloc((void **)&s->v.lv_off[m], sizeof(int) * (size_t)s->cap[m - 1]));
+  }
+  s->scan_cap = maxcap > s->cap_nl ? maxcap : s->cap_nl;
+  if (s->v.nbuckets > s->scan_cap) s->scan_cap = s->v.nbuckets;
+  CK(cudaMalloc((void **)&s->scan_scratch, sizeof(int) * ((size_t)s->scan_cap / 1024 + 64)));
+  s->v.cap_nl = s->cap_nl;
+  return 0;
+}
+
+extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
+  *out = NULL;
+  if (d->natoms <= 0 || d->ninst <= 0) FAIL("empty system");
+  CK(cudaSetDevice(d->device));
+  agb_dev *s = (agb_dev *)calloc(1, sizeof(agb_dev));
+  if (!s) FAIL("out of host memory");
+  s->device = d->device;
+  s->ninst = d->ninst;
+  s->natoms = d->natoms;
+  s->nws = d->nws;
+  s->ntypes = d->ntypes;
+  s->precision = d->precision;
+  s->compat = d->compat;
+  CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  View &v = s->v;
+  memset(&v, 0, sizeof(v));
+  int N = d->natoms, NI = d->ninst, NW = d->nws;
+  v.ninst = NI;
+  v.natoms = N;
+  v.nws = NW;
+  v.ntypes = d->ntypes;
+  v.compat = d->compat;
+
+  s->h_inst_begin = (int *)malloc(sizeof(int) * (NI + 1));
+  s->h_ws_begin = (int *)malloc(sizeof(int) * (NI + 1));
+  memcpy(s->h_inst_begin, d->inst_begin, sizeof(int) * (NI + 1));
+  memcpy(s->h_ws_begin, d->ws_begin, sizeof(int) * (NI + 1));
+
+  /* static per-instance data */
+  int *inst_of = (int *)malloc(sizeof(int) * N);
+  int *bucket_begin = (int *)malloc(sizeof(int) * (NI + 1)), *bucket_mask = (int *)malloc(sizeof(int) * NI);
+  int nb = 0, nheavy_tot = 0;
+  for (int I = 0; I < NI; I++) {
+    for (int g = d->inst_begin[I]; g < d->inst_begin[I + 1]; g++) inst_of[g] = I;
+    int want = 2 * d->inst_nheavy[I], sz = 64;
+    while (sz < want) sz <<= 1;
+    bucket_begin[I] = nb;
+    bucket_mask[I] = sz - 1;
+    nb += sz;
+    nheavy_tot += d->inst_nheavy[I];
+  }
+  bucket_begin[NI] = nb;
+  v.nbuckets = nb;
+  int *ws_inst = (int *)malloc(sizeof(int) * (NW > 0 ? NW : 1));
+  for (int I = 0; I < NI; I++)
+    for (int w = d->ws_begin[I]; w < d->ws_begin[I + 1]; w++) ws_inst[w] = I;
+  double *vols = (double *)malloc(sizeof(double) * N);
+  for (int g = 0; g < N; g++) vols[g] = 4.0 * C_PI / 3.0 * d->r[g] * d->r[g] * d->r[g];
+  size_t ntab = (size_t)d->ntypes * d->ntypes * AGB_NA * 2;
+  float *tabf = (float *)malloc(sizeof(float) * ntab);
+  for (size_t k = 0; k < ntab; k++) tabf[k] = (float)d->tab[k];
+
+#define UP(field, src, n, T)                     \
+  do {                                           \
+    T *p__;                                      \
+    DALLOC(p__, (n), T);                         \
+    if (upload(p__, (src), sizeof(T) * (size_t)(n))) return -1; \
+    v.field = p__;                               \
+  } while (0)
+  UP(inst_begin, d->inst_begin, NI + 1, int);
+  UP(inst_nheavy, d->inst_nheavy, NI, int);
+  UP(inst_of, inst_of, N, int);
+  UP(inst_df, d->inst_df, NI, double);
+  UP(inst_cell, d->inst_cell, NI, float);
+  UP(bucket_begin, bucket_begin, NI + 1, int);
+  UP(bucket_mask, bucket_mask, NI, int);
+  UP(ext_of, d->ext_of, N, int);
+  UP(r, d->r, N, double);
+  UP(charge, d->charge, N, double);
+  UP(igamma, d->igamma, N, double);
+  UP(sgamma, d->sgamma, N, double);
+  UP(ialpha, d->ialpha, N, double);
+  UP(salpha, d->salpha, N, double);
+  UP(vols, vols, N, double);
+  UP(rtype, d->rtype, N, int);
+  UP(tab_d, d->tab, ntab, double);
+  UP(tab_f, tabf, ntab, float);
+  UP(ws_begin, d->ws_begin, NI + 1, int);
+  if (NW > 0) {
+    UP(ws_inst, ws_inst, NW, int);
+    UP(ws_kind, d->ws_kind, NW, int);
+    UP(ws_parent, d->ws_parent, 4 * NW, int);
+    UP(ws_nparent, d->ws_nparent, NW, int);
+    UP(ws_prev, d->ws_prev, NW, int);
+    UP(ws_khb, d->ws_khb, NW, double);
+  }
+  free(inst_of);
+  free(bucket_begin);
+  free(bucket_mask);
+  free(ws_inst);
+  free(vols);
+  free(tabf);
+
+  /* per-evaluation buffers */
+  DALLOC(v.x_ext, N, double);
+  DALLOC(v.y_ext, N, double);
+  DALLOC(v.z_ext, N, double);
+  DALLOC(v.pos, N, f4);
+  DALLOC(v.pxd, N, double);
+  DALLOC(v.pyd, N, double);
+  DALLOC(v.pzd, N, double);
+  DALLOC(v.atom_cell, 3 * N, int);
+  DALLOC(v.atom_bucket, N, int);
+  DALLOC(v.bucket_count, nb, int);
+  DALLOC(v.bucket_start, nb, int);
+  DALLOC(v.bucket_cursor, nb, int);
+  DALLOC(v.cell_atoms, N, int);
+  DALLOC(v.nl_count, N, int);
+  DALLOC(v.nl_off, N, int);
+  DALLOC(v.lv_cnt[2], N, int);
+  DALLOC(v.lv_off[2], N, int);
+  DALLOC(v.dc, DC_SIZE, int);
+  double **dbl[] = {&v.volumep, &v.surf, &v.surf_f, &v.sp, &v.spe, &v.psvol, &v.gammap, &v.bfil, &v.bder,
+                    &v.br, &v.brw, &v.dera, &v.q2ab, &v.abrw, &v.deru, &v.derv, &v.derh, &v.derus, &v.dervs,
+                    &v.o_sp, &v.o_br, &v.o_sa};
+  for (size_t k = 0; k < sizeof(dbl) / sizeof(dbl[0]); k++) DALLOC(*dbl[k], N, double);
+  DALLOC(v.g_gb, 3 * N, double);
+  DALLOC(v.g_vw, 3 * N, double);
+  DALLOC(v.g_cav, 3 * N, double);
+  DALLOC(v.g_hb, 3 * N, double);
+  DALLOC(v.o_gb, 3 * N, double);
+  DALLOC(v.o_gv, 3 * N, double);
+  DALLOC(v.o_gc, 3 * N, double);
+  DALLOC(v.o_gh, 3 * N, double);
+  DALLOC(v.eatom, 7 * N, double);
+  DALLOC(v.ews, NW > 0 ? NW : 1, double);
+  DALLOC(v.wsp, NW > 0 ? NW : 1, double);
+  {
+    void *p;
+    if (dev_alloc(s, &p, sizeof(double) * 3 * (size_t)(NW > 0 ? NW : 1))) return -1;
+    v.wpos = p;
+    if (dev_alloc(s, &p, sizeof(double) * 36 * (size_t)(NW > 0 ? NW : 1))) return -1;
+    v.wdpos = p;
+  }
+  DALLOC(s->esum, 7 * NI, double);
+  DALLOC(s->ehb_inst, NI, double);
+  DALLOC(s->o_energy, 7 * NI, double);
+
+  int dc0[DC_SIZE];
+  memset(dc0, 0, sizeof(dc0));
+  dc0[DC_N] = N;
+  dc0[DC_NB] = nb;
+  dc0[DC_NWS] = NW;
+  if (upload(v.dc, dc0, sizeof(dc0))) return -1;
+
+  /* capacities: kept overlaps per heavy atom at 0.05 atoms/A^3 are ~13,
+     28, 19, 5 for orders 2..5 and ~24 near neighbours; start at a few
+     times that and grow on overflow */
+  s->cap_nl = 48 * nheavy_tot + 4096;
+  s->cap[2] = 32 * nheavy_tot + 4096;
+  s->cap[3] = 64 * nheavy_tot + 4096;
+  s->cap[4] = 64 * nheavy_tot + 4096;
+  s->cap[5] = 32 * nheavy_tot + 4096;
+  if (tree_alloc(s)) return -1;
+  for (int k = 0; k <= AGB_NSTAGE; k++) CK(cudaEventCreate(&s->ev[k]));
+  *out = s;
+  return 0;
+}
+
+extern "C" void agb_dev_destroy(agb_dev *s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  cudaStreamSynchronize(s->st);
+  if (s->graph_ok) cudaGraphExecDestroy(s->gexec);
+  tree_free(s);
+  for (int k = 0; k < s->nallocs; k++) cudaFree(s->allocs[k]);
+  for (int k = 0; k <= AGB_NSTAGE; k++)
+    if (s->ev[k]) cudaEventDestroy(s->ev[k]);
+  cudaStreamDestroy(s->st);
+  free(s->h_inst_begin);
+  free(s->h_ws_begin);
+  free(s);
+}
+
+extern "C" int agb_dev_set_mode(agb_dev *s, int precision, int compat) {
+  if (precision != AGB_PREC_FP64 && precision != AGB_PREC_MIXED) FAIL("unknown precision mode %d", precision);
+  if (s->graph_ok && (precision != s->precision || (compat != 0) != (s->compat != 0))) {
+    cudaGraphExecDestroy(s->gexec);
+    s->graph_ok = 0;
+  }
+  s->precision = precision;
+  s->compat = compat != 0;
+  s->v.compat = s->compat;
+  return 0;
+}
+
+extern "C" int agb_dev_upload_coords(agb_dev *s, const double *x, const double *y, const double *z) {
+  CK(cudaSetDevice(s->device));
+  size_t b = sizeof(double) * s->natoms;
+  CK(cudaMemcpyAsync((void *)s->v.x_ext, x, b, cudaMemcpyHostToDevice, s->st));
+  CK(cudaMemcpyAsync((void *)s->v.y_ext, y, b, cudaMemcpyHostToDevice, s->st));
+  CK(cudaMemcpyAsync((void *)s->v.z_ext, z, b, cudaMemcpyHostToDevice, s->st));
+  return 0;
+}
+
+static inline int nblocks(long long n) {
+  long long b = (n + BLK - 1) / BLK;
+  if (b < 1) b = 1;
+  if (b > 148 * 64) b = 148 * 64;
+  return (int)b;
+}
+
+static void stage_mark(agb_dev *s, int k) {
+  if (s->timing) cudaEventRecord(s->ev[k], s->st);
+}
+
+/* the whole evaluation as a fixed launch sequence */
+template <typename R>
+static void launch_all(agb_dev *s) {
+  View v = s->v;
+  cudaStream_t st = s->st;
+  int N = s->natoms;
+  long long nl = 0;
+  stage_mark(s, 0);
+  cudaMemsetAsync(v.bucket_count, 0, sizeof(int) * v.nbuckets, st);
+  cudaMemsetAsync(v.bucket_cursor, 0, sizeof(int) * v.nbuckets, st);
+  cudaMemsetAsync(v.dc + DC_ERR, 0, sizeof(int), st);
+  AGB_LAUNCH(k_prep, nblocks(N), BLK, st, v);
+  nl += 1;
+  stage_mark(s, 1);
+  AGB_LAUNCH(k_cell_count, nblocks(N), BLK, st, v);
+  agb_scan_excl(v.bucket_count, v.bucket_start, v.dc + DC_NB, v.dc + DC_C0 + 7, v.nbuckets, s->scan_scratch, st);
+  AGB_LAUNCH(k_cell_fill, nblocks(N), BLK, st, v);
+  AGB_LAUNCH(k_nl_count, nblocks(N), BLK, st, v);
+  agb_scan_excl(v.nl_count, v.nl_off, v.dc + DC_N, v.dc + DC_NL, N, s->scan_scratch, st);
+  AGB_LAUNCH(k_nl_emit, nblocks(N), BLK, st, v);
+  nl += 4 + 6;
+  stage_mark(s, 2);
+  AGB_LAUNCH(k_l2_count<R>, nblocks(N), BLK, st, v);
+  agb_scan_excl(v.lv_cnt[2], v.lv_off[2], v.dc + DC_N, v.dc + DC_L0 + 2, N, s->scan_scratch, st);
+  AGB_LAUNCH(k_l2_emit<R>, nblocks(N), BLK, st, v);
+  nl += 2 + 3;
+  for (int m = 3; m <= AGB_MAX_ORDER; m++) {
+    AGB_LAUNCH(k_lm_count<R>, nblocks(v.cap[m - 1]), BLK, st, v, m);
+    agb_scan_excl(v.lv_cnt[m], v.lv_off[m], v.dc + DC_L0 + m - 1, v.dc + DC_L0 + m, v.cap[m - 1], s->scan_scratch,
+                  st);
+    AGB_LAUNCH(k_lm_emit<R>, nblocks(v.cap[m - 1]), BLK, st, v, m);
+    nl += 2 + 3;
+  }
+  stage_mark(s, 3);
+  AGB_LAUNCH(k_scaling, nblocks(N), BLK, st, v);
+  nl += 1;
+  stage_mark(s, 4);
+  AGB_LAUNCH(k_descreen<R>, nblocks(N), BLK, st, v);
+  nl += 1;
+  stage_mark(s, 5);
+  AGB_LAUNCH(k_gbpair<R>, nblocks(N), BLK, st, v);
+  nl += 1;
+  stage_mark(s, 6);
+  AGB_LAUNCH(k_gbders<R>, nblocks(N), BLK, st, v);
+  nl += 1;
+  stage_mark(s, 7);
+  if (s->nws > 0) {
+    AGB_LAUNCH(k_ws_geom<R>, nblocks(s->nws), BLK, st, v);
+    AGB_LAUNCH(k_ws_free<R>, nblocks(s->nws), BLK, st, v);
+    nl += 2;
+  }
+  stage_mark(s, 8);
+  for (int m = 2; m <= AGB_MAX_ORDER; m++) {
+    AGB_LAUNCH(k_tree_ders<R>, nblocks(v.cap[m]), BLK, st, v, m);
+    nl += 1;
+  }
+  stage_mark(s, 9);
+  AGB_LAUNCH(k_final, nblocks(N), BLK, st, v);
+  agb_segment_sum(v.eatom, N, 7, v.inst_begin, s->ninst, s->esum, st);
+  if (s->nws > 0)
+    agb_segment_sum(v.ews, 0, 1, v.ws_begin, s->ninst, s->ehb_inst, st);
+  else
+    cudaMemsetAsync(s->ehb_inst, 0, sizeof(double) * s->ninst, st);
+  AGB_LAUNCH(k_energies, 1, 128, st, s->esum, s->ehb_inst, s->ninst, s->o_energy, v.dc);
+  nl += 4;
+  stage_mark(s, 10);
+  s->nlaunch = nl;
+}
+
+static int run_once(agb_dev *s) {
+  if (s->timing) {
+    if (s->precision == AGB_PREC_FP64)
+      launch_all<double>(s);
+    else
+      launch_all<float>(s);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->st));
+    for (int k = 0; k < 10; k++) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, s->ev[k], s->ev[k + 1]);
+      s->stage_ms[k] = ms;
+    }
+    return 0;
+  }
+  if (!s->graph_ok) {
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+    if (s->precision == AGB_PREC_FP64)
+      launch_all<double>(s);
+    else
+      launch_all<float>(s);
+    CK(cudaStreamEndCapture(s->st, &graph));
+    CK(cudaGraphInstantiate(&s->gexec, graph, 0));
+    cudaGraphDestroy(graph);
+    s->graph_ok = 1;
+  }
+  CK(cudaGraphLaunch(s->gexec, s->st));
+  return 0;
+}
+
+extern "C" int agb_dev_evaluate(agb_dev *s) {
+  CK(cudaSetDevice(s->device));
+  for (int attempt = 0; attempt < 6; attempt++) {
+    if (run_once(s)) return -1;
+    int dc[DC_SIZE];
+    CK(cudaMemcpyAsync(dc, s->v.dc, sizeof(dc), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->last_stats[0] = dc[DC_NL];
+    for (int m = 2; m <= AGB_MAX_ORDER; m++) s->last_stats[m - 1] = dc[DC_L0 + m];
+    s->last_stats[6] = s->nws;
+    s->last_stats[7] = dc[DC_ERR];
+    s->last_stats[8] = s->nlaunch;
+    int err = dc[DC_ERR];
+    if (err & AGB_ERR_WS_CAP) FAIL("more than %d heavy atoms within a water site's search radius", WS_MAXC);
+    if (err & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) {
+      /* grow what overflowed and evaluate again */
+      if (dc[DC_NL] > s->cap_nl) s->cap_nl = 2 * dc[DC_NL];
+      for (int m = 2; m <= AGB_MAX_ORDER; m++)
+        if (dc[DC_L0 + m] > s->cap[m]) s->cap[m] = 2 * dc[DC_L0 + m];
+      if (s->graph_ok) {
+        cudaGraphExecDestroy(s->gexec);
+        s->graph_ok = 0;
+      }
+      tree_free(s);
+      if (tree_alloc(s)) return -1;
+      continue;
+    }
+    if (err & AGB_ERR_NONFINITE) FAIL("non-finite energy");
+    return 0;
+  }
+  FAIL("overlap buffers did not converge after regrowing");
+}
+
+extern "C" int agb_dev_download(agb_dev *s, double *energies, double *sp, double *br, double *surf_area,
+                                double *dgbdr, double *dvwdr, double *decav, double *dehb) {
+  CK(cudaSetDevice(s->device));
+  size_t n = sizeof(double) * s->natoms;
+  View &v = s->v;
+  if (energies) CK(cudaMemcpyAsync(energies, s->o_energy, sizeof(double) * 7 * s->ninst, cudaMemcpyDeviceToHost, s->st));
+  if (sp) CK(cudaMemcpyAsync(sp, v.o_sp, n, cudaMemcpyDeviceToHost, s->st));
+  if (br) CK(cudaMemcpyAsync(br, v.o_br, n, cudaMemcpyDeviceToHost, s->st));
+  if (surf_area) CK(cudaMemcpyAsync(surf_area, v.o_sa, n, cudaMemcpyDeviceToHost, s->st));
+  if (dgbdr) CK(cudaMemcpyAsync(dgbdr, v.o_gb, 3 * n, cudaMemcpyDeviceToHost, s->st));
+  if (dvwdr) CK(cudaMemcpyAsync(dvwdr, v.o_gv, 3 * n, cudaMemcpyDeviceToHost, s->st));
+  if (decav) CK(cudaMemcpyAsync(decav, v.o_gc, 3 * n, cudaMemcpyDeviceToHost, s->st));
+  if (dehb) CK(cudaMemcpyAsync(dehb, v.o_gh, 3 * n, cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return 0;
+}
+
+extern "C" void *agb_dev_stream(agb_dev *s) { return (void *)s->st; }
+
+extern "C" int agb_dev_set_timing(agb_dev *s, int enable) {
+  s->timing = enable != 0;
+  return 0;
+}
+
+extern "C" int agb_dev_stage_times(agb_dev *s, double *ms, int n) {
+  int k;
+  for (k = 0; k < n && k < 10; k++) ms[k] = s->stage_ms[k];
+  return 10;
+}
+
+extern "C" int agb_dev_stats(agb_dev *s, long long *out, int n) {
+  for (int k = 0; k < n && k < 16; k++) out[k] = s->last_stats[k];
+  return 9;
+}
+
+/* debug fetch ids */
+enum {
+  DBG_NL_COUNT = 0, /* int[natoms] */
+  DBG_NL_LIST,      /* int[nl] */
+  DBG_LEVEL_PAR,    /* + m*16: int[m][cap] order-m parents (first n rows valid) */
+  DBG_ATOM = 100,   /* + k: double[natoms] per-atom array k */
+  DBG_WS_SP = 200,  /* double[nws] */
+  DBG_WS_POS,       /* double[3*nws] */
+};
+
+extern "C" long long agb_dev_debug_fetch(agb_dev *s, int what, void *out, long long cap) {
+  cudaSetDevice(s->device);
+  cudaStreamSynchronize(s->st);
+  View &v = s->v;
+  int N = s->natoms;
+  if (what == DBG_NL_COUNT) {
+    if (cap < N) return -1;
+    cudaMemcpy(out, v.nl_count, sizeof(int) * N, cudaMemcpyDeviceToHost);
+    return N;
+  }
+  if (what == DBG_NL_LIST) {
+    long long n = s->last_stats[0];
+    if (n > cap) return -n;
+    cudaMemcpy(out, v.nl_list, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    return n;
+  }
+  if (what >= DBG_LEVEL_PAR && what < DBG_LEVEL_PAR + 16 * (AGB_MAX_ORDER + 1) && (what - DBG_LEVEL_PAR) % 16 == 0) {
+    int m = (what - DBG_LEVEL_PAR) / 16;
+    if (m < 2 || m > AGB_MAX_ORDER) return -1;
+    long long n = s->last_stats[m - 1];
+    if ((long long)m * n > cap) return -(long long)m * n;
+    int *o = (int *)out;
+    for (int k = 0; k < m; k++) cudaMemcpy(o + k * n, v.par[m] + (size_t)k * s->cap[m], sizeof(int) * n, cudaMemcpyDeviceToHost);
+    return n;
+  }
+  if (what >= DBG_ATOM && what < DBG_ATOM + 32) {
+    double *arrs[] = {v.volumep, v.surf, v.surf_f, v.sp, v.spe, v.psvol, v.gammap, v.bfil, v.bder, v.br, v.brw,
+                      v.dera, v.q2ab, v.abrw, v.deru, v.derv, v.derh, v.derus, v.dervs};
+    int k = what - DBG_ATOM;
+    if (k >= (int)(sizeof(arrs) / sizeof(arrs[0])) || cap < N) return -1;
+    cudaMemcpy(out, arrs[k], sizeof(double) * N, cudaMemcpyDeviceToHost);
+    return N;
+  }
+  if (what == DBG_WS_SP) {
+    if (cap < s->nws) return -1;
+    if (s->nws) cudaMemcpy(out, v.wsp, sizeof(double) * s->nws, cudaMemcpyDeviceToHost);
+    return s->nws;
+  }
+  if (what == DBG_WS_POS) {
+    if (cap < 3LL * s->nws) return -1;
+    if (s->nws == 0) return 0;
+    if (s->precision == AGB_PREC_FP64) {
+      cudaMemcpy(out, v.wpos, sizeof(double) * 3 * s->nws, cudaMemcpyDeviceToHost);
+    } else {
+      float *tmp = (float *)malloc(sizeof(float) * 3 * s->nws);
+      cudaMemcpy(tmp, v.wpos, sizeof(float) * 3 * s->nws, cudaMemcpyDeviceToHost);
+      for (int k = 0; k < 3 * s->nws; k++) ((double *)out)[k] = tmp[k];
+      free(tmp);
+    }
+    return s->nws;
+  }
+  return -1;
+}

@@ -1,0 +1,32 @@
+/*
+ * Launch helpers and device-wide primitives shared by the AGBNP3 kernels.
+ *
+ * Every stage kernel is launched through AGB_LAUNCH with a grid sized from
+ * capacities fixed when the instance is created; kernels read their live
+ * item counts from device memory and walk them grid-stride, so a whole
+ * evaluation is a fixed sequence of launches with no host synchronisation
+ * (and can be captured once into a CUDA graph).
+ */
+#ifndef AGBNP3_LAUNCH_CUH
+#define AGBNP3_LAUNCH_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define AGB_LAUNCH(kernel, grid, block, stream, ...) kernel<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__)
+
+#define AGB_GRID_STRIDE(i, n) \
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)(n); \
+       i += (long long)gridDim.x * blockDim.x)
+
+/* exclusive prefix sum of in[0..*n) into out[0..*n), total into *total.
+   `cap` bounds *n and sizes the grid; scratch holds cap/1024+2 ints.
+   The length is read from device memory. */
+void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s);
+
+/* out[q*nseg + k] = sum of vals[q*stride + j] for j in [seg[k], seg[k+1]),
+   for q < nq; one block per (q, k), fixed reduction order */
+void agb_segment_sum(const double *vals, long long stride, int nq, const int *seg, int nseg, double *out,
+                     cudaStream_t s);
+
+#endif

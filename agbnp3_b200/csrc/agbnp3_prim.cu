@@ -1,0 +1,138 @@
+/*
+ * Device-wide exclusive scan with a device-resident length, and a
+ * deterministic segmented sum.  These are the count -> scan -> emit
+ * backbone of the near-list and overlap-tree stages (no atomics on any
+ * index) and the final per-instance energy reductions.
+ */
+#include "agbnp3_launch.cuh"
+
+#define SCAN_BLOCK 1024
+#define SCAN_ITEMS 4 /* items per thread */
+#define SCAN_TILE (SCAN_BLOCK * SCAN_ITEMS)
+
+/* phase 1: tile sums */
+__global__ void k_scan_tiles(const int *__restrict__ in, const int *__restrict__ n, int *__restrict__ tile_sum) {
+  __shared__ int sh[32];
+  int len = *n;
+  long long base = (long long)blockIdx.x * SCAN_TILE;
+  if (base >= len) return;
+  int s = 0;
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
+    if (i < len) s += in[i];
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) sh[warp] = s;
+  __syncthreads();
+  if (warp == 0) {
+    s = lane < SCAN_BLOCK / 32 ? sh[lane] : 0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) tile_sum[blockIdx.x] = s;
+  }
+}
+
+/* phase 2: exclusive scan of the tile sums in one block; writes the total */
+__global__ void k_scan_tile_sums(int *__restrict__ tile_sum, const int *__restrict__ n, int *__restrict__ total) {
+  __shared__ int sh[32];
+  int len = *n;
+  int ntiles = (len + SCAN_TILE - 1) / SCAN_TILE;
+  int carry = 0;
+  for (int base = 0; base < ntiles; base += SCAN_BLOCK) {
+    int i = base + threadIdx.x;
+    int v = i < ntiles ? tile_sum[i] : 0;
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += t;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int w = sh[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += t;
+      }
+      sh[lane] = w;
+    }
+    __syncthreads();
+    int incl = x + (warp > 0 ? sh[warp - 1] : 0);
+    int chunk = sh[31];
+    if (i < ntiles) tile_sum[i] = carry + incl - v;
+    carry += chunk;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+/* phase 3: scan inside each tile, offset by the tile's prefix */
+__global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, const int *__restrict__ n,
+                             const int *__restrict__ tile_sum) {
+  __shared__ int sh[32];
+  int len = *n;
+  long long base = (long long)blockIdx.x * SCAN_TILE;
+  if (base >= len) return;
+  int v[SCAN_ITEMS];
+  int s = 0;
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
+    v[k] = i < len ? in[i] : 0;
+    s += v[k];
+  }
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
+  }
+  if (lane == 31) sh[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = sh[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += t;
+    }
+    sh[lane] = w;
+  }
+  __syncthreads();
+  int run = tile_sum[blockIdx.x] + x - s + (warp > 0 ? sh[warp - 1] : 0);
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
+    if (i < len) out[i] = run;
+    run += v[k];
+  }
+}
+
+void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s) {
+  int ntiles = (cap + SCAN_TILE - 1) / SCAN_TILE;
+  if (ntiles < 1) ntiles = 1;
+  AGB_LAUNCH(k_scan_tiles, ntiles, SCAN_BLOCK, s, in, n, scratch);
+  AGB_LAUNCH(k_scan_tile_sums, 1, SCAN_BLOCK, s, scratch, n, total);
+  AGB_LAUNCH(k_scan_apply, ntiles, SCAN_BLOCK, s, in, out, n, scratch);
+}
+
+#define SEG_BLOCK 256
+__global__ void k_segment_sum(const double *__restrict__ vals, long long stride, const int *__restrict__ seg,
+                              int nseg, double *__restrict__ out) {
+  __shared__ double sh[SEG_BLOCK];
+  int k = blockIdx.x, q = blockIdx.y;
+  const double *v = vals + (long long)q * stride;
+  double s = 0.0;
+  for (int j = seg[k] + threadIdx.x; j < seg[k + 1]; j += SEG_BLOCK) s += v[j];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = SEG_BLOCK / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[(long long)q * nseg + k] = sh[0];
+}
+
+void agb_segment_sum(const double *vals, long long stride, int nq, const int *seg, int nseg, double *out,
+                     cudaStream_t s) {
+  dim3 grid(nseg, nq);
+  k_segment_sum<<<grid, SEG_BLOCK, 0, s>>>(vals, stride, seg, nseg, out);
+}

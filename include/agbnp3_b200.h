@@ -1,0 +1,83 @@
+/*
+ * Extensions of the AGBNP3 C API for the B200 engine.  None of these has a
+ * counterpart in the reference's agbnp3.h; they expose the engine's
+ * precision modes, device-resident evaluation, batches of instances,
+ * per-stage timers and internals for parity testing.
+ */
+#ifndef AGBNP3_B200_H
+#define AGBNP3_B200_H
+
+#include "agbnp3.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* arithmetic of the pair, overlap and descreening stages */
+#define AGBNP3_PREC_FP64 0  /* every stage in double: the plain FP64 path */
+#define AGBNP3_PREC_MIXED 1 /* float pair/overlap/descreening math, double accumulation (default) */
+
+/* compat = 1 (default) reproduces two behaviours of the reference: the
+   water-site free-volume loop reads spe of the previously processed atom
+   (agbnp3_cpu_simd_kernels.c:2854) and the Q4 spline derivative subtracts
+   its second curvature term (agbnp3_utils.c:250-251).  compat = 0 uses each
+   overlap's own atom and the exact spline derivative, so that forces are
+   exactly -dE/dx. */
+int agbnp3_set_mode(int tag, int precision, int compat);
+int agbnp3_get_mode(int tag, int *precision, int *compat);
+
+/* CUDA device used by instances created afterwards (default: $AGBNP3_DEVICE,
+   else $LOCAL_RANK, else 0) */
+int agbnp3_set_device(int device);
+
+/* copies coordinates (caller order) to the device without evaluating */
+int agbnp3_set_coords(int tag, const double *x, const double *y, const double *z);
+/* evaluates at the coordinates on the device; outputs stay on the device
+   until agbnp3_get_results().  No host<->device copies. */
+int agbnp3_ener_resident(int tag);
+/* copies the outputs of the last evaluation (any pointer may be NULL);
+   energies[7] = egb, evdw, ecorr_vdw, ecav, ecorr_cav, ehb, mol_volume */
+int agbnp3_get_results(int tag, double *energies, double *sp, double *br, double *surf_area, double (*dgbdr)[3],
+                       double (*dvwdr)[3], double (*decav)[3], double (*dehb)[3]);
+
+/* the CUDA stream (cudaStream_t) on which an instance's work runs */
+void *agbnp3_stream(int tag);
+
+/* per-stage device timers (CUDA events) of the next evaluations; stage
+   names follow the reference's ATIMER blocks (agbnp3.c:1266-1279) */
+int agbnp3_stage_timing(int tag, int enable);
+int agbnp3_stage_times(int tag, double *ms, int n);
+const char *agbnp3_stage_name(int stage);
+
+/* counters of the last evaluation: [0] near-list pairs, [1..4] kept overlaps
+   of orders 2..5, [5] unused, [6] water sites, [7] device error word,
+   [8] kernel launches per evaluation */
+int agbnp3_stats(int tag, long long *out, int n);
+
+/* internal arrays of the last evaluation, for parity tests (see
+   agbnp3_dev.cu, DBG_*); returns the element count or a negative value */
+long long agbnp3_debug_fetch(int tag, int what, void *out, long long cap);
+
+/* message of the last error */
+const char *agbnp3_last_error(void);
+
+/* batches: several instances evaluated together in one launch sequence.
+   The members keep their tags; coordinates and outputs are the members'
+   arrays concatenated in member order. */
+int agbnp3_batch_new(int *btag, int ntags, const int *tags);
+int agbnp3_batch_delete(int btag);
+int agbnp3_batch_natoms(int btag);
+int agbnp3_batch_set_coords(int btag, const double *x, const double *y, const double *z);
+int agbnp3_batch_ener_resident(int btag);
+/* energies: [ntags][7] as in agbnp3_get_results */
+int agbnp3_batch_get_results(int btag, double *energies, double *sp, double *br, double *surf_area,
+                             double (*dgbdr)[3], double (*dvwdr)[3], double (*decav)[3], double (*dehb)[3]);
+int agbnp3_batch_set_mode(int btag, int precision, int compat);
+void *agbnp3_batch_stream(int btag);
+int agbnp3_batch_stage_timing(int btag, int enable);
+int agbnp3_batch_stage_times(int btag, double *ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
