@@ -213,11 +213,11 @@ __device__ __forceinline__ R q4(const R *tab, int ntypes, int td, int ts, R d, R
   const R hinv = R((AGB_NA - 1) / C_AMAX);
   R rinv = R(1) / Rs;
   R xh = d * rinv * hinv;
-  int k = (int)xh;
-  if (k > AGB_NA - 2) {
+  if (!(xh >= R(0)) || !(xh < R(AGB_NA - 1))) { /* beyond a = 20 (or NaN): Q4 = 0 */
     dq = R(0);
     return R(0);
   }
+  int k = (int)xh;
   const R *t = tab + ((size_t)(td * ntypes + ts) * AGB_NA + k) * 2;
   R y0 = t[0], c0 = t[1], y1 = t[2], c1 = t[3];
   R A = R(k + 1) - xh, B = xh - R(k);
@@ -1422,6 +1422,14 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   s->cap[3] = 64 * nheavy_tot + 4096;
   s->cap[4] = 64 * nheavy_tot + 4096;
   s->cap[5] = 32 * nheavy_tot + 4096;
+  /* AGBNP3_CAPACITY_SCALE (< 1) starts from smaller buffers, which
+     exercises the overflow detection and regrowth of agb_dev_evaluate */
+  const char *cs = getenv("AGBNP3_CAPACITY_SCALE");
+  if (cs && atof(cs) > 0.0) {
+    double f = atof(cs);
+    s->cap_nl = (int)(s->cap_nl * f) + 1;
+    for (int m = 2; m <= AGB_MAX_ORDER; m++) s->cap[m] = (int)(s->cap[m] * f) + 1;
+  }
   if (tree_alloc(s)) return -1;
   for (int k = 0; k <= AGB_NSTAGE; k++) CK(cudaEventCreate(&s->ev[k]));
   *out = s;

@@ -19,9 +19,9 @@
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)(n); \
        i += (long long)gridDim.x * blockDim.x)
 
-/* exclusive prefix sum of in[0..*n) into out[0..*n), total into *total.
-   `cap` bounds *n and sizes the grid; scratch holds cap/1024+2 ints.
-   The length is read from device memory. */
+/* exclusive prefix sum of in[0..len) into out[0..len), len = min(*n, cap),
+   read from device memory; the sum goes to *total.  `cap` is the size of
+   in/out and sizes the grid; scratch holds cap/1024+2 ints. */
 void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s);
 
 /* out[q*nseg + k] = sum of vals[q*stride + j] for j in [seg[k], seg[k+1]),

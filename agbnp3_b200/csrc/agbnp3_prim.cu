@@ -11,9 +11,9 @@
 #define SCAN_TILE (SCAN_BLOCK * SCAN_ITEMS)
 
 /* phase 1: tile sums */
-__global__ void k_scan_tiles(const int *__restrict__ in, const int *__restrict__ n, int *__restrict__ tile_sum) {
+__global__ void k_scan_tiles(const int *__restrict__ in, const int *__restrict__ n, int cap, int *__restrict__ tile_sum) {
   __shared__ int sh[32];
-  int len = *n;
+  int len = min(*n, cap);
   long long base = (long long)blockIdx.x * SCAN_TILE;
   if (base >= len) return;
   int s = 0;
@@ -33,9 +33,9 @@ __global__ void k_scan_tiles(const int *__restrict__ in, const int *__restrict__
 }
 
 /* phase 2: exclusive scan of the tile sums in one block; writes the total */
-__global__ void k_scan_tile_sums(int *__restrict__ tile_sum, const int *__restrict__ n, int *__restrict__ total) {
+__global__ void k_scan_tile_sums(int *__restrict__ tile_sum, const int *__restrict__ n, int cap, int *__restrict__ total) {
   __shared__ int sh[32];
-  int len = *n;
+  int len = min(*n, cap);
   int ntiles = (len + SCAN_TILE - 1) / SCAN_TILE;
   int carry = 0;
   for (int base = 0; base < ntiles; base += SCAN_BLOCK) {
@@ -68,10 +68,10 @@ __global__ void k_scan_tile_sums(int *__restrict__ tile_sum, const int *__restri
 }
 
 /* phase 3: scan inside each tile, offset by the tile's prefix */
-__global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, const int *__restrict__ n,
+__global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, const int *__restrict__ n, int cap,
                              const int *__restrict__ tile_sum) {
   __shared__ int sh[32];
-  int len = *n;
+  int len = min(*n, cap);
   long long base = (long long)blockIdx.x * SCAN_TILE;
   if (base >= len) return;
   int v[SCAN_ITEMS];
@@ -109,9 +109,9 @@ __global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, 
 void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s) {
   int ntiles = (cap + SCAN_TILE - 1) / SCAN_TILE;
   if (ntiles < 1) ntiles = 1;
-  AGB_LAUNCH(k_scan_tiles, ntiles, SCAN_BLOCK, s, in, n, scratch);
-  AGB_LAUNCH(k_scan_tile_sums, 1, SCAN_BLOCK, s, scratch, n, total);
-  AGB_LAUNCH(k_scan_apply, ntiles, SCAN_BLOCK, s, in, out, n, scratch);
+  AGB_LAUNCH(k_scan_tiles, ntiles, SCAN_BLOCK, s, in, n, cap, scratch);
+  AGB_LAUNCH(k_scan_tile_sums, 1, SCAN_BLOCK, s, scratch, n, cap, total);
+  AGB_LAUNCH(k_scan_apply, ntiles, SCAN_BLOCK, s, in, out, n, cap, scratch);
 }
 
 #define SEG_BLOCK 256

@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""AGBNP3 energy+gradient throughput on B200.
+
+Default workload: one 25,000-atom synthetic globule (seeded generator,
+0.05 heavy atoms/A^3), evaluated in the engine's chosen mode (FP32 pair,
+overlap and descreening math with FP64 accumulation).  A step is one full
+energy+gradient evaluation (agbnp3_ener).  The plain FP64 path is timed in
+the same run for the speed-up and accuracy columns.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With N > 1 (torchrun, one process per GPU) every rank evaluates its own
+conformation (a different seed); no collective touches the data path
+(weak scaling).  --impl reference times the reference's own CPU library
+(oracle/_ref, built from the reference sources) through its public API on
+the same workload with all host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+METRIC = "energy+grad evals/s @25k atoms (chosen mode: FP32 math + FP64 accumulation)"
+UNIT = "evals/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--natoms", type=int, default=25000)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--fp64-steps", type=int, default=5)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed
+    region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------
+# reference arm and CPU baseline: the reference library built from its sources
+# ----------------------------------------------------------------------------
+def _ref_child(natoms, seed, steps, warmup, threads, out_path):
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from agbnp3_b200.system import make_globule
+    s = make_globule(natoms, seed)
+    ref = O.RefLib(harness=False)
+    tag = ref.new(s)
+    times = []
+    for k in range(warmup + steps):
+        t0 = time.perf_counter()
+        r = ref.ener(tag, s)
+        dt = time.perf_counter() - t0
+        if k >= warmup:
+            times.append(dt)
+    json.dump({"times": times, "egb": r["egb"], "rc": r["rc"]}, open(out_path, "w"))
+
+
+def run_reference(natoms, seed, steps, warmup, threads):
+    """Times agbnp3_ener of the reference library in a fresh process (the
+    reference supports one instance per process)."""
+    import multiprocessing as mp
+    import tempfile
+    out = tempfile.NamedTemporaryFile(suffix=".json", delete=False).name
+    ctx = mp.get_context("spawn")
+    p = ctx.Process(target=_ref_child, args=(natoms, seed, steps, warmup, threads, out))
+    p.start()
+    p.join(timeout=3600)
+    if p.exitcode != 0:
+        raise RuntimeError(f"reference run failed (exit {p.exitcode})")
+    d = json.load(open(out))
+    os.unlink(out)
+    return d
+
+
+def reference_arm(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    ref_lib = os.path.join(ROOT, "oracle", "_ref", "libagbnp3_ref.so")
+    cfg = {"workload": f"globule {args.natoms} atoms, seed {args.seed}", "natoms": args.natoms}
+    if not os.path.exists(ref_lib):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libagbnp3_ref.so not built "
+                          "(needs the reference sources at build time)"}))
+        return
+    threads = os.cpu_count() or 1
+    d = run_reference(args.natoms, args.seed, args.steps, args.warmup, threads)
+    tot = sum(d["times"])
+    v = len(d["times"]) / tot
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(d["times"]), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} full evaluations of the {args.natoms}-atom globule"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# ----------------------------------------------------------------------------
+# engine arm
+# ----------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import agbnp3_b200 as A
+    A.lib().agbnp3_set_device(local)
+    A.initialize()
+
+    natoms = args.natoms
+    s = A.make_globule(natoms, args.seed + rank)
+    inst = A.Instance(s, precision=A.PREC_MIXED, compat=True)
+    ref_out = inst.ener()  # sizes the buffers, captures the graph
+    stream = torch.cuda.ExternalStream(inst.stream, device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def timed_resident(obj, steps, warmup):
+        obj.set_coords(s.coords())
+        for _ in range(warmup):
+            obj.ener_resident()
+        times = []
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()  # evicts the 126 MB L2 between steps
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            obj.ener_resident()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return times
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        times = timed_resident(inst, args.steps, args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    tot_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([tot_ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    value = world * args.steps / (tot_ms / 1e3)
+    mixed = inst.results()
+    st = inst.stats()
+
+    # per-stage device times (CUDA events between stages, direct launches)
+    inst.stage_timing(True)
+    stage = {}
+    for _ in range(3):
+        inst.ener_resident()
+        for k, v in inst.stage_times().items():
+            stage.setdefault(k, []).append(v)
+    inst.stage_timing(False)
+    stage_ms = {k: statistics.median(v) for k, v in stage.items()}
+
+    # plain FP64 path: speed and the accuracy of the chosen mode against it
+    inst64 = A.Instance(s, precision=A.PREC_FP64, compat=True)
+    inst64.ener()
+    t64 = timed_resident(inst64, args.fp64_steps, 1)
+    fp64_value = world * len(t64) / (sum(t64) / 1e3)
+    full = inst64.results()
+    inst64.close()
+    tot = lambda R: sum(R[k] for k in ("egb", "evdw", "ecav", "ehb"))  # noqa: E731
+    frc = lambda R: R["dgbdr"] + R["dvwdr"] + R["decav"] + R["dehb"]  # noqa: E731
+    acc = {"energy_rel_err": abs(tot(mixed) - tot(full)) / abs(tot(full)),
+           "force_rms_rel_err": float(np.sqrt(((frc(mixed) - frc(full)) ** 2).sum() / (frc(full) ** 2).sum())),
+           "per_term_rel_err": {k: abs(mixed[k] - full[k]) / max(abs(full[k]), 1e-12)
+                                for k in ("egb", "evdw", "ecav", "ehb", "mol_volume")}}
+
+    # e2e: through agbnp3_ener with host buffers (pinned), copies included
+    L = A.lib()
+    pin = lambda n: torch.empty(n, dtype=torch.float64, pin_memory=True)  # noqa: E731
+    hx, hy, hz = pin(natoms), pin(natoms), pin(natoms)
+    hx.numpy()[:], hy.numpy()[:], hz.numpy()[:] = s.x, s.y, s.z
+    outs = [pin(natoms) for _ in range(3)] + [pin(3 * natoms) for _ in range(4)]
+    import ctypes
+    dptr = lambda t: ctypes.cast(t.data_ptr(), ctypes.POINTER(ctypes.c_double))  # noqa: E731
+    es = [ctypes.c_double() for _ in range(7)]
+
+    def call():
+        rc = L.agbnp3_ener(inst.tag, 0, dptr(hx), dptr(hy), dptr(hz), dptr(outs[0]), dptr(outs[1]),
+                           ctypes.byref(es[6]), dptr(outs[2]), ctypes.byref(es[0]), dptr(outs[3]),
+                           ctypes.byref(es[1]), ctypes.byref(es[2]), dptr(outs[4]), ctypes.byref(es[3]),
+                           ctypes.byref(es[4]), dptr(outs[5]), ctypes.byref(es[5]), dptr(outs[6]))
+        if rc != A.AGBNP_OK:
+            raise RuntimeError(A.last_error())
+
+    for _ in range(args.warmup):
+        call()
+    e2e_t = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        call()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_tot = sum(e2e_t)
+    if world > 1:
+        t = torch.tensor([e2e_tot], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_tot = float(t.item())
+    e2e_value = world * args.steps / e2e_tot
+
+    # dominant stage and its arithmetic rate (pair counts x
+    # frozen per-pair operation weights)
+    nh = s.nheavy
+    pairs = {"agb": natoms * (natoms - 1), "invb": natoms * nh, "gbders": 2 * nh * (natoms - 1)}
+    flops_per_pair = {"agb": 30, "invb": 32, "gbders": 40}
+    dom = max(stage_ms, key=stage_ms.get)
+    roof = None
+    if dom in pairs:
+        achieved = pairs[dom] * flops_per_pair[dom] / (stage_ms[dom] * 1e-3) / 1e12
+        roof = {"kernel": dom, "bound": "fp32", "achieved": achieved, "unit": "TFLOP/s",
+                "peak": None, "frac": None, "traffic": None,
+                "note": "FP32 issue bound; peak from the FP32 FMA microbenchmark when available"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and os.path.exists(os.path.join(ROOT, "oracle", "_ref",
+                                                                             "libagbnp3_ref.so")):
+        try:
+            threads = os.cpu_count() or 1
+            d = run_reference(natoms, args.seed, 1, 0, threads)
+            cpu = {"value": 1.0 / d["times"][0], "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"1 evaluation of the {natoms}-atom globule, reference library, {threads} OpenMP threads"}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 math / f64 accumulation", "data": "synthetic",
+            "config": {"workload": f"globule {natoms} atoms ({s.nheavy} heavy), 0.05 heavy/A^3, seed {args.seed}",
+                       "mode": "mixed", "compat": True, "l2": "256 MB flush between timed steps",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "fp64_plain": {"value": fp64_value, "unit": UNIT, "ms_per_step": sum(t64) / len(t64),
+                           "speedup_of_chosen": value / fp64_value},
+            "accuracy_vs_fp64": acc,
+            "stage_ms": stage_ms,
+            "counts": st,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * natoms,
+                    "d2h_bytes_per_step": (3 + 12) * 8 * natoms + 7 * 8},
+            "gpu_launches": int(st["launches"]) * args.steps,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    inst.close()
+    A.terminate()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,260 @@
+"""Parity of the CUDA engine (called through its C-ABI) with the FP64 oracle
+and with the reference library's golden outputs.
+
+Tolerances:
+- plain FP64 path vs FP64 oracle: energies 1e-9 relative, per-atom outputs
+  and forces 1e-9 RMS relative (only summation order differs);
+- mixed path (float pair/overlap math, double accumulation) vs FP64 oracle:
+  energies 1e-5 relative (or 1e-4 kcal/mol), forces 1e-4 RMS relative;
+- both paths vs the reference's FP32 golden outputs: the FP32 tolerances of
+  tests/test_oracle_golden.py;
+- near lists and kept-overlap index sets: identical.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import ENERGY_KEYS, GOLDEN_CASES, load_golden, rms_rel
+
+pytestmark = pytest.mark.gpu
+
+A = pytest.importorskip("agbnp3_b200")
+
+TOL = {A.PREC_FP64: dict(e=1e-9, g=1e-9), A.PREC_MIXED: dict(e=1e-5, g=1e-4)}
+PREC_NAMES = {A.PREC_FP64: "fp64", A.PREC_MIXED: "mixed"}
+
+
+def check_vs_oracle(R, Q, prec, label=""):
+    t = TOL[prec]
+    for k in ENERGY_KEYS:
+        assert abs(R[k] - Q[k]) <= t["e"] * max(abs(Q[k]), 10.0), (label, k, R[k], Q[k])
+    for k in ("sp", "br", "surf_area"):
+        assert rms_rel(R[k], Q[k]) <= t["g"], (label, k, rms_rel(R[k], Q[k]))
+    for k in ("dgbdr", "dvwdr", "decav", "dehb"):
+        assert rms_rel(R[k], Q[k]) <= t["g"], (label, k, rms_rel(R[k], Q[k]))
+
+
+@pytest.fixture(scope="module")
+def engine():
+    A.initialize()
+    yield A
+    A.terminate()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+@pytest.mark.parametrize("compat", [True, False], ids=["compat", "exact"])
+def test_engine_vs_oracle(engine, name, prec, compat):
+    s, _ = load_golden(name)
+    inst = A.Instance(s, precision=prec, compat=compat)
+    try:
+        R = inst.ener()
+        check_vs_oracle(R, O.oracle_eval(s, compat=compat), prec, f"{name}/{PREC_NAMES[prec]}")
+    finally:
+        inst.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_engine_vs_reference_golden(engine, name, prec):
+    """Through agbnp3_ener, against the reference library's own outputs."""
+    s, d = load_golden(name)
+    inst = A.Instance(s, precision=prec, compat=True)
+    try:
+        R = inst.ener()
+        for k, ref in zip(ENERGY_KEYS, d["energies"]):
+            assert abs(R[k] - ref) <= 2e-5 * max(abs(ref), 1.0), (name, k, R[k], ref)
+        for k in ("sp", "br", "surf_area"):
+            assert rms_rel(R[k], d[k]) < 2e-5, (name, k)
+        for k in ("dgbdr", "dvwdr", "decav", "dehb"):
+            assert rms_rel(R[k], d[k]) < 1e-4, (name, k, rms_rel(R[k], d[k]))
+    finally:
+        inst.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_near_list_bit_exact(engine, name, prec):
+    """Heavy-atom near list: same pairs in the same (float d^2, index)
+    order as the reference (agbnp3.c:4041-4066)."""
+    s, d = load_golden(name)
+    inst = A.Instance(s, precision=prec)
+    try:
+        inst.ener()
+        cnt, lst = inst.near_list()
+        assert np.array_equal(cnt[: s.nheavy], d["nl_count"])
+        assert np.array_equal(lst, d["nl_list"])
+    finally:
+        inst.close()
+
+
+def canonical(parents):
+    return {tuple(sorted(p)) for p in parents.tolist()}
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_overlap_sets(engine, name, prec):
+    """Kept overlaps of every order: the same index sets as the oracle,
+    whose candidates equal the reference's (test_oracle_golden).  Any
+    difference may only involve overlaps whose volume sits on the switch's
+    lower edge."""
+    s, d = load_golden(name)
+    n = int(d["ncand"])
+    Q = O.oracle_eval(s, internals=True, cand_cap=n + 10)
+    c = Q["cand"]
+    int2ext, ext2int = s.internal_order()
+    inst = A.Instance(s, precision=prec)
+    try:
+        inst.ener()
+        for m in range(2, 6):
+            sel = (c["order"] == m) & (c["gvolp"] > np.finfo(np.float32).tiny)
+            want = canonical(c["parents"][sel, :m])
+            got = canonical(inst.overlaps(m))
+            diff = want ^ got
+            if diff:
+                border = {tuple(sorted(p)) for p, g in zip(c["parents"][c["order"] == m, :m].tolist(),
+                                                          c["gvol"][c["order"] == m]) if abs(g - 0.01) < 1e-5}
+                assert diff <= border, (m, len(diff))
+    finally:
+        inst.close()
+
+
+def test_resident_graph_matches_direct(engine):
+    """Graph replay of the device-resident path gives the same outputs as
+    agbnp3_ener, and repeated replays are consistent."""
+    s, _ = load_golden("globule300_shuffled")
+    inst = A.Instance(s, precision=A.PREC_MIXED)
+    try:
+        R = inst.ener()
+        inst.set_coords(s.coords())
+        for _ in range(3):
+            inst.ener_resident()
+        G = inst.results()
+        for k in ENERGY_KEYS:
+            assert abs(G[k] - R[k]) <= 1e-9 * max(1.0, abs(R[k]))
+        for k in ("dgbdr", "dehb"):
+            assert rms_rel(G[k], R[k]) < 1e-9
+    finally:
+        inst.close()
+
+
+def test_batch_matches_members(engine):
+    """A batch of uneven instances evaluates each member as if alone."""
+    systems = [A.make_globule(n, seed, noise=0.2) for n, seed in ((300, 1), (777, 2), (1500, 3), (420, 4))]
+    insts = [A.Instance(x, precision=A.PREC_MIXED) for x in systems]
+    B = A.Batch(insts)
+    try:
+        B.set_coords(np.concatenate([x.coords() for x in systems]))
+        B.ener_resident()
+        R = B.results()
+        for k, (x, inst) in enumerate(zip(systems, insts)):
+            S = inst.ener()
+            o0, o1 = B.offsets[k], B.offsets[k + 1]
+            for e in ENERGY_KEYS:
+                assert abs(R[e][k] - S[e]) <= 1e-9 * max(1.0, abs(S[e])), (k, e)
+            for g in ("dgbdr", "dvwdr", "decav", "dehb"):
+                assert rms_rel(R[g][o0:o1], S[g]) < 1e-9, (k, g)
+    finally:
+        B.close()
+        for i in insts:
+            i.close()
+
+
+def test_caller_order_and_permutation(engine):
+    """Outputs follow the caller's atom order: a renumbered molecule gives
+    the same per-atom values, renumbered."""
+    s, _ = load_golden("globule300_shuffled")
+    perm = np.random.default_rng(5).permutation(s.natoms)
+    a, b = A.Instance(s, precision=A.PREC_FP64), A.Instance(s.permuted(perm), precision=A.PREC_FP64)
+    try:
+        Ra, Rb = a.ener(), b.ener()
+        for k in ENERGY_KEYS:
+            assert abs(Ra[k] - Rb[k]) <= 1e-9 * max(1.0, abs(Ra[k]))
+        for k in ("br", "sp", "dgbdr", "dehb"):
+            assert rms_rel(Rb[k], Ra[k][perm]) < 1e-9
+    finally:
+        a.close()
+        b.close()
+
+
+def test_edge_cases(engine):
+    """Two atoms, a molecule without hydrogens, and coincident atoms."""
+    s = A.make_globule(60, 9)
+    # no hydrogens: keep the heavy atoms only
+    heavy = np.setdiff1d(np.arange(s.natoms), s.ihydrogen)
+    keep = {int(h): i for i, h in enumerate(heavy)}
+    bonds = np.array([[keep[a], keep[b]] for a, b in s.bonds if a in keep and b in keep], dtype=np.int32)
+    sh = A.System(x=s.x[heavy], y=s.y[heavy], z=s.z[heavy], r=s.r[heavy], charge=s.charge[heavy],
+                  igamma=s.igamma[heavy], sgamma=s.sgamma[heavy], ialpha=s.ialpha[heavy], salpha=s.salpha[heavy],
+                  hbtype=np.where(s.hbtype[heavy] == 1, 0, s.hbtype[heavy]).astype(np.int32),
+                  hbcorr=s.hbcorr[heavy], ihydrogen=np.zeros(0, np.int32), bonds=bonds)
+    two = A.System(x=np.array([0.0, 3.0]), y=np.zeros(2), z=np.zeros(2), r=np.array([1.7, 1.52]),
+                   charge=np.array([0.3, -0.3]), igamma=np.full(2, 0.117), sgamma=np.zeros(2),
+                   ialpha=np.full(2, -0.05), salpha=np.zeros(2), hbtype=np.array([0, 20], np.int32),
+                   hbcorr=np.full(2, -0.7), ihydrogen=np.zeros(0, np.int32), bonds=np.array([[0, 1]], np.int32))
+    for sys_ in (sh, two):
+        for prec in (A.PREC_FP64, A.PREC_MIXED):
+            inst = A.Instance(sys_, precision=prec)
+            try:
+                check_vs_oracle(inst.ener(), O.oracle_eval(sys_), prec, "edge")
+            finally:
+                inst.close()
+    # coincident heavy atoms: finite energies, pair excluded from GB
+    c = A.make_globule(80, 11)
+    c.x[1], c.y[1], c.z[1] = c.x[0], c.y[0], c.z[0]
+    inst = A.Instance(c, precision=A.PREC_FP64)
+    try:
+        R = inst.ener()
+        assert all(np.isfinite(R[k]) for k in ENERGY_KEYS)
+        assert np.isfinite(R["dgbdr"]).all()
+    finally:
+        inst.close()
+
+
+def test_api_errors_on_device(engine):
+    s, _ = load_golden("globule50")
+    with pytest.raises(A.AGBNPError):
+        A.new(s, conntbl=False)
+    tag = A.new(s)
+    A.delete(tag)
+    with pytest.raises(A.AGBNPError):
+        A.ener(tag, s.x, s.y, s.z)
+    with pytest.raises(A.AGBNPError):
+        A.delete(tag)
+
+
+@pytest.mark.parametrize("natoms,seed", [(25000, 1)])
+def test_large_fp64_vs_oracle(engine, natoms, seed):
+    """The benchmark workload (25,000-atom globule): plain FP64 path against
+    the FP64 oracle, and the mixed path within the model's accuracy targets
+    (energy 1e-4 relative, forces 1e-3 RMS relative)."""
+    s = A.make_globule(natoms, seed)
+    Q = O.oracle_eval(s, compat=True)
+    a = A.Instance(s, precision=A.PREC_FP64)
+    b = A.Instance(s, precision=A.PREC_MIXED)
+    try:
+        Ra, Rb = a.ener(), b.ener()
+        check_vs_oracle(Ra, Q, A.PREC_FP64, "25k/fp64")
+        et = lambda R: sum(R[k] for k in ("egb", "evdw", "ecav", "ehb"))  # noqa: E731
+        assert abs(et(Rb) - et(Q)) <= 1e-4 * abs(et(Q))
+        ft = lambda R: R["dgbdr"] + R["dvwdr"] + R["decav"] + R["dehb"]  # noqa: E731
+        assert rms_rel(ft(Rb), ft(Q)) <= 1e-3
+    finally:
+        a.close()
+        b.close()
+
+
+def test_capacity_regrowth(engine, monkeypatch):
+    """Near-list and overlap buffers that start far too small overflow, are
+    detected through the device error word, regrown and the evaluation is
+    repeated with identical results."""
+    s, _ = load_golden("globule300_shuffled")
+    q = O.oracle_eval(s)
+    monkeypatch.setenv("AGBNP3_CAPACITY_SCALE", "0.001")
+    inst = A.Instance(s, precision=A.PREC_FP64)
+    try:
+        check_vs_oracle(inst.ener(), q, A.PREC_FP64, "regrowth")
+        assert inst.stats()["error"] == 0
+    finally:
+        inst.close()
