@@ -56,7 +56,6 @@
 #define C_RW 1.4
 #define C_TOKCAL 332.0
 #define C_AMAX 20.0
-#define WS_MAXC 256 /* heavy atoms within a water site's search radius */
 
 #define BLK 128
 
@@ -103,9 +102,15 @@ struct View {
   double *wsp;                        /* [nws] */
   double *o_sp, *o_br, *o_sa, *o_gb, *o_gv, *o_gc, *o_gh;
   int nbuckets;
+  void *pa[12];      /* packed pair-stage operands (R[natoms] each) */
+  int *nl_c27, *nl_o27; /* near-list counts / offsets per (atom, neighbour cell) */
+  int *ws_c27, *ws_o27, *ws_cand; /* water-site candidates per (site, cell) */
+  int cap_wsc;
+  double *acc_beta; /* descreening sums */
 };
 
-enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m */, DC_C0 = DC_L0 + 8 /* candidates */ };
+enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m */, DC_C0 = DC_L0 + 8 /* scratch */,
+       DC_N27 = DC_C0 + 2, DC_W27, DC_WSC };
 #define DC_SIZE (DC_C0 + 8)
 
 /* record fields of a kept overlap */
@@ -300,26 +305,6 @@ __global__ void k_cell_fill(View v) {
   }
 }
 
-/* visits the heavy atoms of instance I in the 27 cells around cell c;
-   an atom is taken only from its own cell, so hash collisions never yield
-   duplicates.  fn(j) is called once per atom. */
-template <typename Fn>
-__device__ __forceinline__ void for_cell_neighbours(const View &v, int I, int cx, int cy, int cz, Fn fn) {
-  int mask = v.bucket_mask[I], base = v.bucket_begin[I];
-  for (int dz = -1; dz <= 1; dz++)
-    for (int dy = -1; dy <= 1; dy++)
-      for (int dx = -1; dx <= 1; dx++) {
-        int ax = cx + dx, ay = cy + dy, az = cz + dz;
-        int b = base + cell_hash(ax, ay, az, mask);
-        int s0 = v.bucket_start[b], s1 = s0 + v.bucket_count[b];
-        for (int s = s0; s < s1; s++) {
-          int j = v.cell_atoms[s];
-          if (v.atom_cell[3 * j] != ax || v.atom_cell[3 * j + 1] != ay || v.atom_cell[3 * j + 2] != az) continue;
-          fn(j);
-        }
-      }
-}
-
 /* the reference's float membership test d^2 < (1.6 (ri + rj))^2, evaluated
    without fused operations (agbnp3.c:4041-4049) */
 __device__ __forceinline__ bool near_test(const f4 &a, const f4 &b, float &d2) {
@@ -329,50 +314,83 @@ __device__ __forceinline__ bool near_test(const f4 &a, const f4 &b, float &d2) {
   return d2 < __fmul_rn(u, u);
 }
 
-__global__ void k_nl_count(View v) {
-  AGB_GRID_STRIDE(g, v.natoms) {
+/* the heavy atoms of instance I in cell (ax, ay, az): fn(j) once each */
+template <typename Fn>
+__device__ __forceinline__ void for_cell(const View &v, int I, int ax, int ay, int az, Fn fn) {
+  int b = v.bucket_begin[I] + cell_hash(ax, ay, az, v.bucket_mask[I]);
+  int s0 = v.bucket_start[b], s1 = s0 + v.bucket_count[b];
+  for (int s = s0; s < s1; s++) {
+    int j = v.cell_atoms[s];
+    if (v.atom_cell[3 * j] != ax || v.atom_cell[3 * j + 1] != ay || v.atom_cell[3 * j + 2] != az) continue;
+    fn(j);
+  }
+}
+
+/* one thread per (heavy atom, neighbour cell): near partners j > i */
+__global__ void k_nl_count27(View v) {
+  AGB_GRID_STRIDE(q, 27LL * v.natoms) {
+    int g = (int)(q / 27), c = (int)(q % 27);
     int I = v.inst_of[g];
     int cnt = 0;
     if (g < v.inst_begin[I] + v.inst_nheavy[I]) {
       f4 a = v.pos[g];
-      for_cell_neighbours(v, I, v.atom_cell[3 * g], v.atom_cell[3 * g + 1], v.atom_cell[3 * g + 2], [&](int j) {
-        float d2;
-        if (j > g && near_test(a, v.pos[j], d2)) cnt++;
-      });
+      for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
+               v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j) {
+                 float d2;
+                 if (j > g && near_test(a, v.pos[j], d2)) cnt++;
+               });
     }
-    v.nl_count[g] = cnt;
+    v.nl_c27[q] = cnt;
   }
 }
 
-__global__ void k_nl_emit(View v) {
-  AGB_GRID_STRIDE(g, v.natoms) {
-    int n = v.nl_count[g];
+__global__ void k_nl_emit27(View v) {
+  AGB_GRID_STRIDE(q, 27LL * v.natoms) {
+    int n = v.nl_c27[q];
     if (n == 0) continue;
-    int o = v.nl_off[g];
+    int o = v.nl_o27[q];
     if (o + n > v.cap_nl) {
       set_err(v, AGB_ERR_NL_CAP);
       continue;
     }
+    int g = (int)(q / 27), c = (int)(q % 27);
     int I = v.inst_of[g];
     f4 a = v.pos[g];
     int m = 0;
-    int *lst = v.nl_list + o;
-    float *dd = v.nl_d2 + o;
-    for_cell_neighbours(v, I, v.atom_cell[3 * g], v.atom_cell[3 * g + 1], v.atom_cell[3 * g + 2], [&](int j) {
-      float d2;
-      if (j > g && near_test(a, v.pos[j], d2) && m < n) {
-        /* insertion into the (d^2, index)-sorted prefix
-           (agbnp3.c:3766-3792, 4062-4066) */
-        int k = m++;
-        while (k > 0 && (dd[k - 1] > d2 || (dd[k - 1] == d2 && lst[k - 1] > j))) {
-          dd[k] = dd[k - 1];
-          lst[k] = lst[k - 1];
-          k--;
-        }
-        dd[k] = d2;
-        lst[k] = j;
+    for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
+             v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j) {
+               float d2;
+               if (j > g && near_test(a, v.pos[j], d2) && m < n) {
+                 v.nl_list[o + m] = j;
+                 v.nl_d2[o + m] = d2;
+                 m++;
+               }
+             });
+  }
+}
+
+/* each atom's list in (float d^2, index) order (agbnp3.c:3766-3792,
+   4062-4066), and the per-atom CSR of the near list */
+__global__ void k_nl_sort(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int o = v.nl_o27[27 * g], e = (g + 1 < v.natoms) ? v.nl_o27[27 * (g + 1)] : v.dc[DC_NL];
+    v.nl_off[g] = o;
+    v.nl_count[g] = e - o;
+    if (e > v.cap_nl) continue;
+    int *lst = v.nl_list;
+    float *dd = v.nl_d2;
+    for (int a = o + 1; a < e; a++) {
+      int j = lst[a];
+      float d2 = dd[a];
+      int k = a;
+      while (k > o && (dd[k - 1] > d2 || (dd[k - 1] == d2 && lst[k - 1] > j))) {
+        dd[k] = dd[k - 1];
+        lst[k] = lst[k - 1];
+        k--;
       }
-    });
+      dd[k] = d2;
+      lst[k] = j;
+    }
   }
 }
 
@@ -559,29 +577,157 @@ __global__ void k_scaling(View v) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* invb: descreening -> Born radii, vdW energy                              */
+/* packed per-atom operands of the pair stages, in the working precision    */
 /* ------------------------------------------------------------------------ */
+enum { PA_X = 0, PA_Y, PA_Z, PA_RINV, PA_RH, PA_SP, PA_W, PA_Q, PA_B, PA_BINV, PA_Q2AB, PA_ABRW, PA_NUM };
+
 template <typename R>
-__global__ void k_descreen(View v) {
-  const R *tab = tables<R>(v);
+__device__ __forceinline__ R *pa(const View &v, int k) {
+  return (R *)v.pa[k];
+}
+
+template <typename R>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  typedef float2 T;
+};
+template <>
+struct Vec2<double> {
+  typedef double2 T;
+};
+
+template <typename R>
+__device__ __forceinline__ const typename Vec2<R>::T *tables2(const View &v) {
+  return (const typename Vec2<R>::T *)tables<R>(v);
+}
+
+/* exp(-d^2 / (4 Bi Bj)) as exp2 of a pre-scaled argument in float */
+template <typename R>
+struct GbExp;
+template <>
+struct GbExp<float> {
+  static __device__ __forceinline__ float scale() { return -0.25f * 1.4426950408889634f; }
+  static __device__ __forceinline__ float ex(float a) { return exp2f(a); }
+};
+template <>
+struct GbExp<double> {
+  static __device__ __forceinline__ double scale() { return -0.25; }
+  static __device__ __forceinline__ double ex(double a) { return exp(a); }
+};
+
+/* cubic spline of one Q4 table at xh = a / h in [0, AGB_NA-1): value and,
+   optionally, d/da (agbnp3_utils.c:229-252) */
+template <typename R>
+__device__ __forceinline__ R spline(const typename Vec2<R>::T *tab, int slot, R xh, R &fp, bool want_fp,
+                                    bool ref_sign) {
+  const R h = R(C_AMAX / (AGB_NA - 1)), hinv = R((AGB_NA - 1) / C_AMAX);
+  const R dp1 = h * R(1.0 / 6.0), dp2 = h * dp1;
+  int k = (int)xh;
+  const typename Vec2<R>::T *t = tab + (size_t)slot * AGB_NA + k;
+  typename Vec2<R>::T t0 = __ldg(t), t1 = __ldg(t + 1);
+  R B = xh - R(k), A = R(1) - B;
+  R f = A * t0.x + B * t1.x + (A * (A * A - R(1)) * t0.y + B * (B * B - R(1)) * t1.y) * dp2;
+  if (want_fp) {
+    R c1 = (R(3) * B * B - R(1)) * t1.y;
+    fp = (t1.x - t0.x) * hinv - ((R(3) * A * A - R(1)) * t0.y + (ref_sign ? c1 : -c1)) * dp1;
+  }
+  return f;
+}
+
+template <typename R>
+__global__ void k_pack_geom(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    R ri = R(1) / (R)v.r[g];
+    pa<R>(v, PA_X)[g] = px<R>(v, (int)g);
+    pa<R>(v, PA_Y)[g] = py<R>(v, (int)g);
+    pa<R>(v, PA_Z)[g] = pz<R>(v, (int)g);
+    pa<R>(v, PA_RINV)[g] = ri;
+    pa<R>(v, PA_RH)[g] = ri * R((AGB_NA - 1) / C_AMAX);
+    pa<R>(v, PA_Q)[g] = (R)v.charge[g];
+    v.acc_beta[g] = 0.0;
+  }
+}
+
+template <typename R>
+__global__ void k_pack_sp(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    R sp = (R)v.sp[g];
+    pa<R>(v, PA_SP)[g] = sp;
+    pa<R>(v, PA_W)[g] = sp * pa<R>(v, PA_RINV)[g];
+  }
+}
+
+/* partner range of a work item: chunk w.w of nch of [p0, p1) */
+__device__ __forceinline__ void chunk_range(int p0, int p1, int c, int nch, int &c0, int &c1) {
+  long long len = p1 - p0;
+  c0 = p0 + (int)(len * c / nch);
+  c1 = p0 + (int)(len * (c + 1) / nch);
+}
+
+/* ------------------------------------------------------------------------ */
+/* invb: descreening sums (agbnp3_cpu_simd_kernels.c:500-678).  Each block  */
+/* owns up to ITILE atoms of one instance and one chunk of its heavy        */
+/* descreeners, staged through shared memory; per-tile sums in R are added  */
+/* to a double accumulator.                                                 */
+/* ------------------------------------------------------------------------ */
+#define ITILE 128
+
+template <typename R>
+__global__ void __launch_bounds__(ITILE) k_descreen_t(View v, const int4 *__restrict__ items, int nitems,
+                                                      int nch) {
+  AGB_SHARED R sx[ITILE], sy[ITILE], sz[ITILE], srh[ITILE], sw[ITILE];
+  AGB_SHARED int st[ITILE];
+  const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
+  const R *RH = pa<R>(v, PA_RH), *W = pa<R>(v, PA_W);
+  const typename Vec2<R>::T *tab = tables2<R>(v);
+  const int nt = v.ntypes;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    int4 w = items[it];
+    int g = w.y + threadIdx.x;
+    bool act = g < w.z;
+    int p0 = v.inst_begin[w.x], c0, c1;
+    chunk_range(p0, p0 + v.inst_nheavy[w.x], w.w, nch, c0, c1);
+    R xg = act ? X[g] : R(0), yg = act ? Y[g] : R(0), zg = act ? Z[g] : R(0);
+    int row = act ? v.rtype[g] * nt : 0;
+    double acc = 0.0;
+    for (int j0 = c0; j0 < c1; j0 += ITILE) {
+      int n = min(ITILE, c1 - j0);
+      AGB_SYNC();
+      AGB_COOP_FOR(t, n) {
+        sx[t] = X[j0 + t];
+        sy[t] = Y[j0 + t];
+        sz[t] = Z[j0 + t];
+        srh[t] = RH[j0 + t];
+        sw[t] = W[j0 + t];
+        st[t] = v.rtype[j0 + t];
+      }
+      AGB_SYNC();
+      if (act) {
+        R part = R(0);
+        for (int t = 0; t < n; t++) {
+          R dx = sx[t] - xg, dy = sy[t] - yg, dz = sz[t] - zg;
+          R xh = m_sqrt(dx * dx + dy * dy + dz * dz) * srh[t];
+          if (xh < R(AGB_NA - 1) && j0 + t != g) {
+            R fp;
+            part += sw[t] * spline<R>(tab, row + st[t], xh, fp, false, false);
+          }
+        }
+        acc += (double)part;
+      }
+    }
+    if (act) atomicAdd(&v.acc_beta[g], acc);
+  }
+}
+
+/* inverse Born radius, its filter, Born radius, vdW energy
+   (agbnp3_cpu_simd_kernels.c:605, agbnp3.c:1174-1188, 1466-1487,
+   agbnp3_utils.c:615-670) */
+template <typename R>
+__global__ void k_born(View v) {
   size_t N = v.natoms;
   AGB_GRID_STRIDE(g, v.natoms) {
-    int I = v.inst_of[g];
-    int h0 = v.inst_begin[I], h1 = h0 + v.inst_nheavy[I];
-    R xg = px<R>(v, (int)g), yg = py<R>(v, (int)g), zg = pz<R>(v, (int)g);
-    int tg = v.rtype[g];
-    double acc = 0.0;
-    for (int h = h0; h < h1; h++) {
-      if (h == g) continue;
-      R dx = px<R>(v, h) - xg, dy = py<R>(v, h) - yg, dz = pz<R>(v, h) - zg;
-      R d = m_sqrt(dx * dx + dy * dy + dz * dz);
-      R dq;
-      R q = q4<R>(tab, v.ntypes, tg, v.rtype[h], d, (R)v.r[h], dq, false, false);
-      acc += (double)(q * (R)v.sp[h]);
-    }
-    /* inverse Born radius, its filter and the Born radius
-       (agbnp3_cpu_simd_kernels.c:605, agbnp3.c:1174-1188) */
-    double beta = 1.0 / (v.r[g] - C_RINC) - acc / (4.0 * C_PI);
+    double beta = 1.0 / (v.r[g] - C_RINC) - v.acc_beta[g] / (4.0 * C_PI);
     double bf, bd;
     if (beta < 0.0) {
       bf = 0.02;
@@ -598,116 +744,226 @@ __global__ void k_descreen(View v) {
     double a3 = 1.0 / (t * t * t);
     v.eatom[2 * N + g] = v.ialpha[g] * a3;
     v.eatom[3 * N + g] = v.salpha[g] * a3;
+    v.eatom[N + g] = 0.0;
+    v.dera[g] = 0.0;
+    pa<R>(v, PA_B)[g] = (R)b;
+    pa<R>(v, PA_BINV)[g] = (R)bf;
   }
 }
 
 /* ------------------------------------------------------------------------ */
-/* agb: GB pair energy, gradient at constant Born radii, A_i                */
+/* agb: GB pair energy, gradient at constant Born radii and A_i             */
+/* (agbnp3_cpu_simd_kernels.c:66-151, 329-460), all ordered pairs           */
 /* ------------------------------------------------------------------------ */
 template <typename R>
-__global__ void k_gbpair(View v) {
+__global__ void __launch_bounds__(ITILE) k_agb_t(View v, const int4 *__restrict__ items, int nitems, int nch) {
+  AGB_SHARED R sx[ITILE], sy[ITILE], sz[ITILE], sq[ITILE], sb[ITILE], sbi[ITILE];
+  const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
+  const R *Q = pa<R>(v, PA_Q), *Bv = pa<R>(v, PA_B), *BI = pa<R>(v, PA_BINV);
   size_t N = v.natoms;
-  AGB_GRID_STRIDE(g, v.natoms) {
-    int I = v.inst_of[g];
-    int j0 = v.inst_begin[I], j1 = v.inst_begin[I + 1];
-    double df = v.inst_df[I];
-    R xi = px<R>(v, (int)g), yi = py<R>(v, (int)g), zi = pz<R>(v, (int)g);
-    R qi = (R)v.charge[g], bi = (R)v.br[g];
-    R qf = R(2.0 * df);
-    double e = 0.0, at = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-    for (int j = j0; j < j1; j++) {
-      R dx = px<R>(v, j) - xi, dy = py<R>(v, j) - yi, dz = pz<R>(v, j) - zi;
-      R d2 = dx * dx + dy * dy + dz * dz;
-      if (!(d2 > R(0))) continue; /* the pair itself and coincident atoms */
-      R qq = qi * (R)v.charge[j];
-      R bb = bi * (R)v.br[j];
-      R et = m_exp(R(-0.25) * d2 / bb);
-      R f = m_rsqrt(d2 + bb * et);
-      R f3 = f * f * f;
-      R w = qf * qq;
-      e += (double)(w * f);
-      R mw = -w * (R(1) - R(0.25) * et) * f3;
-      gx -= (double)(mw * dx);
-      gy -= (double)(mw * dy);
-      gz -= (double)(mw * dz);
-      at += (double)(qq * (bb + R(0.25) * d2) * et * f3);
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    int4 w = items[it];
+    int g = w.y + threadIdx.x;
+    bool act = g < w.z;
+    int c0, c1;
+    chunk_range(v.inst_begin[w.x], v.inst_begin[w.x + 1], w.w, nch, c0, c1);
+    double df = v.inst_df[w.x];
+    R xg = act ? X[g] : R(0), yg = act ? Y[g] : R(0), zg = act ? Z[g] : R(0);
+    R bg = act ? Bv[g] : R(1), cg = act ? GbExp<R>::scale() * BI[g] : R(0);
+    double e = 0, gx = 0, gy = 0, gz = 0, at = 0;
+    for (int j0 = c0; j0 < c1; j0 += ITILE) {
+      int n = min(ITILE, c1 - j0);
+      AGB_SYNC();
+      AGB_COOP_FOR(t, n) {
+        sx[t] = X[j0 + t];
+        sy[t] = Y[j0 + t];
+        sz[t] = Z[j0 + t];
+        sq[t] = Q[j0 + t];
+        sb[t] = Bv[j0 + t];
+        sbi[t] = BI[j0 + t];
+      }
+      AGB_SYNC();
+      if (act) {
+        R pe = 0, px_ = 0, py_ = 0, pz_ = 0, pat = 0;
+        for (int t = 0; t < n; t++) {
+          R dx = sx[t] - xg, dy = sy[t] - yg, dz = sz[t] - zg;
+          R d2 = dx * dx + dy * dy + dz * dz;
+          if (!(d2 > R(0))) continue; /* the atom itself and coincident atoms */
+          R bb = bg * sb[t];
+          R et = GbExp<R>::ex(cg * sbi[t] * d2);
+          R f = m_rsqrt(d2 + bb * et);
+          R qf3 = sq[t] * f * f * f;
+          pe += sq[t] * f;
+          R mw = (R(1) - R(0.25) * et) * qf3;
+          px_ += mw * dx;
+          py_ += mw * dy;
+          pz_ += mw * dz;
+          pat += (bb + R(0.25) * d2) * et * qf3;
+        }
+        e += (double)pe;
+        gx += (double)px_;
+        gy += (double)py_;
+        gz += (double)pz_;
+        at += (double)pat;
+      }
     }
+    if (act) {
+      /* qj and the factor 2 df qi are applied once per atom */
+      double qi = v.charge[g], w2 = 2.0 * df * qi;
+      atomicAdd(&v.eatom[N + g], C_TOKCAL * 0.5 * w2 * e);
+      atomicAdd(&v.g_gb[3 * g], w2 * gx);
+      atomicAdd(&v.g_gb[3 * g + 1], w2 * gy);
+      atomicAdd(&v.g_gb[3 * g + 2], w2 * gz);
+      atomicAdd(&v.dera[g], qi * at);
+    }
+  }
+}
+
+/* self energy, q2ab and abrw (agbnp3_cpu_simd_kernels.c:359, 444-449) */
+template <typename R>
+__global__ void k_agb_post(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    double df = v.inst_df[v.inst_of[g]];
     double q = v.charge[g], b = v.br[g];
-    v.g_gb[3 * g] += gx;
-    v.g_gb[3 * g + 1] += gy;
-    v.g_gb[3 * g + 2] += gz;
-    v.dera[g] = at;
     v.eatom[g] = C_TOKCAL * df * q * q / b;
-    v.eatom[N + g] = C_TOKCAL * 0.5 * e;
-    /* agbnp3_cpu_simd_kernels.c:444-449 */
-    v.q2ab[g] = (q * q + at * b) * v.bder[g];
-    v.abrw[g] = (v.ialpha[g] + v.salpha[g]) * v.brw[g] * v.bder[g];
+    double q2ab = (q * q + v.dera[g] * b) * v.bder[g];
+    double abrw = (v.ialpha[g] + v.salpha[g]) * v.brw[g] * v.bder[g];
+    v.q2ab[g] = q2ab;
+    v.abrw[g] = abrw;
+    pa<R>(v, PA_Q2AB)[g] = (R)q2ab;
+    pa<R>(v, PA_ABRW)[g] = (R)abrw;
+    v.deru[g] = v.derv[g] = 0.0;
   }
 }
 
 /* ------------------------------------------------------------------------ */
-/* gbders: gradient through the Born radii at constant self volumes, U, V   */
+/* gbders: GB and vdW gradients through the Born radii at constant self      */
+/* volumes and U_i, V_i (agbnp3_cpu_simd_kernels.c:681-904).  Thread a adds  */
+/* for each partner b the pair force of both descreening directions; U_a,    */
+/* V_a collect the atoms a descreens.                                        */
 /* ------------------------------------------------------------------------ */
 template <typename R>
-__global__ void k_gbders(View v) {
-  const R *tab = tables<R>(v);
+__global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restrict__ items, int nitems,
+                                                    int nch) {
+  AGB_SHARED R sx[ITILE], sy[ITILE], sz[ITILE], srh[ITILE], sri[ITILE], ssp[ITILE], sq2[ITILE], sab[ITILE];
+  AGB_SHARED int st[ITILE];
+  const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
+  const R *RH = pa<R>(v, PA_RH), *RI = pa<R>(v, PA_RINV), *SP = pa<R>(v, PA_SP);
+  const R *Q2 = pa<R>(v, PA_Q2AB), *AB = pa<R>(v, PA_ABRW);
+  const typename Vec2<R>::T *tab = tables2<R>(v);
+  const int nt = v.ntypes;
   const bool rs = v.compat != 0;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    int4 w = items[it];
+    int g = w.y + threadIdx.x;
+    bool act = g < w.z;
+    int a0 = v.inst_begin[w.x], hh = a0 + v.inst_nheavy[w.x], a1 = v.inst_begin[w.x + 1];
+    /* a tile of hydrogens only needs heavy partners */
+    int c0, c1;
+    chunk_range(a0, w.y >= hh ? hh : a1, w.w, nch, c0, c1);
+    bool heavy = g < hh;
+    R xg = act ? X[g] : R(0), yg = act ? Y[g] : R(0), zg = act ? Z[g] : R(0);
+    R rhg = act ? RH[g] : R(0), rig = act ? RI[g] : R(0), spg = act ? SP[g] : R(0);
+    R q2g = act ? Q2[g] : R(0), abg = act ? AB[g] : R(0);
+    int tg = act ? v.rtype[g] : 0;
+    double U = 0, V = 0, fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
+    for (int j0 = c0; j0 < c1; j0 += ITILE) {
+      int n = min(ITILE, c1 - j0);
+      AGB_SYNC();
+      AGB_COOP_FOR(t, n) {
+        sx[t] = X[j0 + t];
+        sy[t] = Y[j0 + t];
+        sz[t] = Z[j0 + t];
+        srh[t] = RH[j0 + t];
+        sri[t] = RI[j0 + t];
+        ssp[t] = SP[j0 + t];
+        sq2[t] = Q2[j0 + t];
+        sab[t] = AB[j0 + t];
+        st[t] = v.rtype[j0 + t];
+      }
+      AGB_SYNC();
+      if (act) {
+        R pu = 0, pv = 0, pfx = 0, pfy = 0, pfz = 0, pvx = 0, pvy = 0, pvz = 0;
+        int tend = heavy ? n : min(n, hh - j0); /* hydrogens: heavy partners only */
+        for (int t = 0; t < tend; t++) {
+          int b = j0 + t;
+          R dx = sx[t] - xg, dy = sy[t] - yg, dz = sz[t] - zg;
+          R d2 = dx * dx + dy * dy + dz * dz;
+          if (!(d2 > R(0))) continue;
+          R id = m_rsqrt(d2);
+          R d = d2 * id;
+          R ht = R(0), ut = R(0);
+          if (heavy) { /* b descreened by a: table (type b, type a), radius of a */
+            R xh = d * rhg;
+            if (xh < R(AGB_NA - 1)) {
+              R fp;
+              R f = spline<R>(tab, st[t] * nt + tg, xh, fp, true, rs);
+              R q = f * rig, dq = fp * rig * rig;
+              pu += sq2[t] * q;
+              pv += sab[t] * q;
+              ht += sq2[t] * dq * spg;
+              ut += sab[t] * dq * spg;
+            }
+          }
+          if (b < hh) { /* a descreened by b: table (type a, type b), radius of b */
+            R xh = d * srh[t];
+            if (xh < R(AGB_NA - 1)) {
+              R fp;
+              spline<R>(tab, tg * nt + st[t], xh, fp, true, rs);
+              R dq = fp * sri[t] * sri[t] * ssp[t];
+              ht += q2g * dq;
+              ut += abg * dq;
+            }
+          }
+          ht *= id;
+          ut *= id;
+          pfx += ht * dx;
+          pfy += ht * dy;
+          pfz += ht * dz;
+          pvx += ut * dx;
+          pvy += ut * dy;
+          pvz += ut * dz;
+        }
+        U += (double)pu;
+        V += (double)pv;
+        fx += (double)pfx;
+        fy += (double)pfy;
+        fz += (double)pfz;
+        vx += (double)pvx;
+        vy += (double)pvy;
+        vz += (double)pvz;
+      }
+    }
+    if (act) {
+      const double f4p = 1.0 / (4.0 * C_PI);
+      double kg = f4p * v.inst_df[w.x];
+      atomicAdd(&v.g_gb[3 * g], kg * fx);
+      atomicAdd(&v.g_gb[3 * g + 1], kg * fy);
+      atomicAdd(&v.g_gb[3 * g + 2], kg * fz);
+      atomicAdd(&v.g_vw[3 * g], f4p * vx);
+      atomicAdd(&v.g_vw[3 * g + 1], f4p * vy);
+      atomicAdd(&v.g_vw[3 * g + 2], f4p * vz);
+      if (heavy) {
+        atomicAdd(&v.deru[g], U);
+        atomicAdd(&v.derv[g], V);
+      }
+    }
+  }
+}
+
+/* U_i, V_i normalised by the atomic volume and the surface-area effective
+   gammas (agbnp3_cpu_simd_kernels.c:861-874) */
+__global__ void k_gbders_post(View v) {
   AGB_GRID_STRIDE(g, v.natoms) {
     int I = v.inst_of[g];
-    int h0 = v.inst_begin[I], hh = h0 + v.inst_nheavy[I], j1 = v.inst_begin[I + 1];
-    bool heavy = g < hh;
-    double df = v.inst_df[I];
-    R xa = px<R>(v, (int)g), ya = py<R>(v, (int)g), za = pz<R>(v, (int)g);
-    int ta = v.rtype[g];
-    R ra = (R)v.r[g], spa = (R)v.sp[g];
-    R q2a = (R)v.q2ab[g], aba = (R)v.abrw[g];
-    double u = 0.0, w = 0.0, gbx = 0, gby = 0, gbz = 0, gvx = 0, gvy = 0, gvz = 0;
-    int jend = heavy ? j1 : hh; /* hydrogens are only descreened */
-    for (int b = h0; b < jend; b++) {
-      if (b == g) continue;
-      R dx = px<R>(v, b) - xa, dy = py<R>(v, b) - ya, dz = pz<R>(v, b) - za;
-      R d = m_sqrt(dx * dx + dy * dy + dz * dz);
-      if (!(d > R(0))) continue;
-      R ht = R(0), ut = R(0);
-      if (heavy) { /* b descreened by a */
-        R dq;
-        R q = q4<R>(tab, v.ntypes, v.rtype[b], ta, d, ra, dq, true, rs);
-        R q2b = (R)v.q2ab[b], abb = (R)v.abrw[b];
-        u += (double)(q2b * q);
-        w += (double)(abb * q);
-        ht += q2b * dq * spa;
-        ut += abb * dq * spa;
-      }
-      if (b < hh) { /* a descreened by b */
-        R dq;
-        q4<R>(tab, v.ntypes, ta, v.rtype[b], d, (R)v.r[b], dq, true, rs);
-        R spb = (R)v.sp[b];
-        ht += q2a * dq * spb;
-        ut += aba * dq * spb;
-      }
-      R id = R(1) / d;
-      double hs = (double)(ht * id), us = (double)(ut * id);
-      gbx += hs * (double)dx;
-      gby += hs * (double)dy;
-      gbz += hs * (double)dz;
-      gvx += us * (double)dx;
-      gvy += us * (double)dy;
-      gvz += us * (double)dz;
-    }
-    const double f4p = 1.0 / (4.0 * C_PI);
-    v.g_gb[3 * g] += f4p * df * gbx;
-    v.g_gb[3 * g + 1] += f4p * df * gby;
-    v.g_gb[3 * g + 2] += f4p * df * gbz;
-    v.g_vw[3 * g] += f4p * gvx;
-    v.g_vw[3 * g + 1] += f4p * gvy;
-    v.g_vw[3 * g + 2] += f4p * gvz;
-    if (heavy) { /* agbnp3_cpu_simd_kernels.c:861-874 */
+    if (g < v.inst_begin[I] + v.inst_nheavy[I]) {
+      const double f4p = 1.0 / (4.0 * C_PI);
       double vol = v.vols[g];
-      double du = u / vol, dv = w / vol;
+      double du = v.deru[g] / vol, dv = v.derv[g] / vol;
       v.deru[g] = du;
       v.derv[g] = dv;
       v.dervs[g] = f4p * v.psvol[g] * dv;
-      v.derus[g] = df * f4p * v.psvol[g] * du;
+      v.derus[g] = v.inst_df[I] * f4p * v.psvol[g] * du;
     } else {
       v.deru[g] = v.derv[g] = v.dervs[g] = v.derus[g] = 0.0;
     }
@@ -944,54 +1200,81 @@ __global__ void k_ws_geom(View v) {
 /* ------------------------------------------------------------------------ */
 /* ws: free volumes, HB energy and gradient                                 */
 /* ------------------------------------------------------------------------ */
+/* heavy atoms within 1.6 (r + 1.4) of a water site, one thread per
+   (site, neighbour cell) (agbnp3_cpu_simd_kernels.c:2786-2811) */
+template <typename R>
+__device__ __forceinline__ int ws_cell_scan(const View &v, int w, int c, int *out, int cap) {
+  const R *wpos = (const R *)v.wpos;
+  int I = v.ws_inst[w];
+  R px_ = wpos[3 * w], py_ = wpos[3 * w + 1], pz_ = wpos[3 * w + 2];
+  float inv = 1.0f / v.inst_cell[I];
+  int cx, cy, cz;
+  cell_of((float)px_, (float)py_, (float)pz_, inv, cx, cy, cz);
+  int m = 0;
+  for_cell(v, I, cx + c % 3 - 1, cy + (c / 3) % 3 - 1, cz + c / 9 - 1, [&](int h) {
+    R dx = px<R>(v, h) - px_, dy = py<R>(v, h) - py_, dz = pz<R>(v, h) - pz_;
+    R u = ((R)v.r[h] + R(C_HBRAD)) * R(1.6);
+    if (dx * dx + dy * dy + dz * dz < u * u) {
+      if (out && m < cap) out[m] = h;
+      m++;
+    }
+  });
+  return m;
+}
+
+template <typename R>
+__global__ void k_ws_count27(View v) {
+  AGB_GRID_STRIDE(q, 27LL * v.nws) { v.ws_c27[q] = ws_cell_scan<R>(v, (int)(q / 27), (int)(q % 27), NULL, 0); }
+}
+
+template <typename R>
+__global__ void k_ws_emit27(View v) {
+  AGB_GRID_STRIDE(q, 27LL * v.nws) {
+    int n = v.ws_c27[q], o = v.ws_o27[q];
+    if (n == 0) continue;
+    if (o + n > v.cap_wsc) {
+      set_err(v, AGB_ERR_WS_CAP);
+      continue;
+    }
+    ws_cell_scan<R>(v, (int)(q / 27), (int)(q % 27), v.ws_cand + o, n);
+  }
+}
+
+/* free volumes, HB energy and gradient (agbnp3_cpu_simd_kernels.c:
+   2831-2933): the candidates of a site in heavy-atom index order, spe-
+   weighted overlaps subtracted until the free volume drops to 60% */
 template <typename R>
 __global__ void k_ws_free(View v) {
   const R *wpos = (const R *)v.wpos, *wd = (const R *)v.wdpos;
   const R vw = R(4.0 / 3.0 * C_PI * C_HBRAD * C_HBRAD * C_HBRAD);
   const R aw = R(C_KFC / (C_HBRAD * C_HBRAD));
   AGB_GRID_STRIDE(w, v.nws) {
-    int I = v.ws_inst[w];
-    V3<R> p = {wpos[3 * w], wpos[3 * w + 1], wpos[3 * w + 2]};
-    int cand[WS_MAXC];
-    int nc = 0;
-    bool over = false;
-    float inv = 1.0f / v.inst_cell[I];
-    int cx, cy, cz;
-    cell_of((float)p.x, (float)p.y, (float)p.z, inv, cx, cy, cz);
-    /* heavy atoms with d^2 < (1.6 (r + 1.4))^2, in index order
-       (agbnp3_cpu_simd_kernels.c:2786-2811) */
-    for_cell_neighbours(v, I, cx, cy, cz, [&](int h) {
-      R dx = px<R>(v, h) - p.x, dy = py<R>(v, h) - p.y, dz = pz<R>(v, h) - p.z;
-      R u = ((R)v.r[h] + R(C_HBRAD)) * R(1.6);
-      if (dx * dx + dy * dy + dz * dz < u * u) {
-        if (nc == WS_MAXC) {
-          over = true;
-          return;
-        }
-        int k = nc++;
-        while (k > 0 && cand[k - 1] > h) {
-          cand[k] = cand[k - 1];
-          k--;
-        }
-        cand[k] = h;
+    if (v.dc[DC_ERR] & AGB_ERR_WS_CAP) continue;
+    int o = v.ws_o27[27 * w], e = (w + 1 < v.nws) ? v.ws_o27[27 * (w + 1)] : v.dc[DC_WSC];
+    int *cand = v.ws_cand + o;
+    int nc = e - o;
+    for (int a = 1; a < nc; a++) { /* index order */
+      int h = cand[a], k = a;
+      while (k > 0 && cand[k - 1] > h) {
+        cand[k] = cand[k - 1];
+        k--;
       }
-    });
-    if (over) set_err(v, AGB_ERR_WS_CAP);
-    /* free volume: subtract spe-weighted overlaps in index order until the
-       free volume drops to 60% (agbnp3_cpu_simd_kernels.c:2831-2895) */
+      cand[k] = h;
+    }
+    V3<R> p = {wpos[3 * w], wpos[3 * w + 1], wpos[3 * w + 2]};
     double fv = (double)vw, cut = C_HBSWA0 * (double)vw;
     int prev = v.ws_prev[w];
     int np = 0;
     for (int c = 0; c < nc; c++) {
       if (!(fv > cut)) break;
       int h = cand[c];
-      Ov<R> o = ogauss<R>(aw, R(C_PFC), p.x, p.y, p.z, atom_alpha<R>(v, h), R(C_PFC), px<R>(v, h), py<R>(v, h),
-                          pz<R>(v, h));
-      if (!(o.gvolp > R(0))) continue;
+      Ov<R> ov = ogauss<R>(aw, R(C_PFC), p.x, p.y, p.z, atom_alpha<R>(v, h), R(C_PFC), px<R>(v, h), py<R>(v, h),
+                           pz<R>(v, h));
+      if (!(ov.gvolp > R(0))) continue;
       double s_used = v.compat ? (prev >= 0 ? v.spe[prev] : 0.0) : v.spe[h];
-      fv -= s_used * (double)o.gvolp;
+      fv -= s_used * (double)ov.gvolp;
       prev = h;
-      cand[np++] = h;
+      cand[np++] = h; /* processed overlaps, compacted in place */
     }
     double spw = fv / (double)vw, fp, fpp;
     double sw = poly_switch<double>(spw, C_HBSWA, C_HBSWB, fp, fpp);
@@ -999,22 +1282,21 @@ __global__ void k_ws_free(View v) {
     double dhw = khb * fp / (double)vw;
     v.ews[w] = khb * sw;
     v.wsp[w] = spw;
-    /* derivatives (agbnp3_cpu_simd_kernels.c:2904-2933) */
     double jw[3] = {0, 0, 0};
     for (int c = 0; c < np; c++) {
       int h = cand[c];
       R ah = atom_alpha<R>(v, h);
-      Ov<R> o = ogauss<R>(aw, R(C_PFC), p.x, p.y, p.z, ah, R(C_PFC), px<R>(v, h), py<R>(v, h), pz<R>(v, h));
+      Ov<R> ov = ogauss<R>(aw, R(C_PFC), p.x, p.y, p.z, ah, R(C_PFC), px<R>(v, h), py<R>(v, h), pz<R>(v, h));
       double sh = v.spe[h];
-      double fi = -2.0 * (double)(ah * o.gvol * o.fp), fw = -2.0 * (double)(aw * o.gvol * o.fp);
+      double fi = -2.0 * (double)(ah * ov.gvol * ov.fp), fw = -2.0 * (double)(aw * ov.gvol * ov.fp);
       double uu = -sh * dhw;
-      atomicAdd(&v.g_hb[3 * h], uu * fi * (double)(px<R>(v, h) - o.cx));
-      atomicAdd(&v.g_hb[3 * h + 1], uu * fi * (double)(py<R>(v, h) - o.cy));
-      atomicAdd(&v.g_hb[3 * h + 2], uu * fi * (double)(pz<R>(v, h) - o.cz));
-      atomicAdd(&v.derh[h], dhw / v.vols[h] * (double)o.gvolp);
-      jw[0] += uu * fw * (double)(p.x - o.cx);
-      jw[1] += uu * fw * (double)(p.y - o.cy);
-      jw[2] += uu * fw * (double)(p.z - o.cz);
+      atomicAdd(&v.g_hb[3 * h], uu * fi * (double)(px<R>(v, h) - ov.cx));
+      atomicAdd(&v.g_hb[3 * h + 1], uu * fi * (double)(py<R>(v, h) - ov.cy));
+      atomicAdd(&v.g_hb[3 * h + 2], uu * fi * (double)(pz<R>(v, h) - ov.cz));
+      atomicAdd(&v.derh[h], dhw / v.vols[h] * (double)ov.gvolp);
+      jw[0] += uu * fw * (double)(p.x - ov.cx);
+      jw[1] += uu * fw * (double)(p.y - ov.cy);
+      jw[2] += uu * fw * (double)(p.z - ov.cz);
     }
     int npar = v.ws_nparent[w];
     for (int q = 0; q < npar; q++) {
@@ -1186,7 +1468,7 @@ struct agb_dev {
   void *allocs[128];
   int nallocs;
   /* tree capacity (owned separately, regrown on overflow) */
-  int cap_nl, cap[AGB_MAX_ORDER + 1];
+  int cap_nl, cap[AGB_MAX_ORDER + 1], cap_wsc;
   int *scan_scratch;
   int scan_cap;
   double *esum, *ehb_inst, *o_energy;
@@ -1198,6 +1480,8 @@ struct agb_dev {
   double stage_ms[AGB_NSTAGE];
   long long nlaunch;
   long long last_stats[16];
+  int4 *items; /* (instance, first atom, end atom, partner chunk) */
+  int nitems, nch;
 };
 
 static int dev_alloc(agb_dev *s, void **p, size_t bytes) {
@@ -1236,6 +1520,8 @@ static int tree_free(agb_dev *s) {
     if (s->v.lv_off[m]) cudaFree(s->v.lv_off[m]);
     s->v.lv_cnt[m] = s->v.lv_off[m] = NULL;
   }
+  if (s->v.ws_cand) cudaFree(s->v.ws_cand);
+  s->v.ws_cand = NULL;
   if (s->v.nl_list) cudaFree(s->v.nl_list);
   if (s->v.nl_d2) cudaFree(s->v.nl_d2);
   if (s->scan_scratch) cudaFree(s->scan_scratch);
@@ -1247,6 +1533,8 @@ static int tree_free(agb_dev *s) {
 
 static int tree_alloc(agb_dev *s) {
   size_t rsz = sizeof(double); /* records sized for the wider type */
+  CK(cudaMalloc((void **)&s->v.ws_cand, sizeof(int) * (size_t)s->cap_wsc));
+  s->v.cap_wsc = s->cap_wsc;
   CK(cudaMalloc((void **)&s->v.nl_list, sizeof(int) * (size_t)s->cap_nl));
   CK(cudaMalloc((void **)&s->v.nl_d2, sizeof(float) * (size_t)s->cap_nl));
   int maxcap = s->natoms;
@@ -1264,6 +1552,8 @@ static int tree_alloc(agb_dev *s) {
   }
   s->scan_cap = maxcap > s->cap_nl ? maxcap : s->cap_nl;
   if (s->v.nbuckets > s->scan_cap) s->scan_cap = s->v.nbuckets;
+  if (27 * s->natoms > s->scan_cap) s->scan_cap = 27 * s->natoms;
+  if (27 * s->nws > s->scan_cap) s->scan_cap = 27 * s->nws;
   CK(cudaMalloc((void **)&s->scan_scratch, sizeof(int) * ((size_t)s->scan_cap / 1024 + 64)));
   s->v.cap_nl = s->cap_nl;
   return 0;
@@ -1378,6 +1668,10 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   DALLOC(v.cell_atoms, N, int);
   DALLOC(v.nl_count, N, int);
   DALLOC(v.nl_off, N, int);
+  DALLOC(v.nl_c27, 27 * N, int);
+  DALLOC(v.nl_o27, 27 * N, int);
+  DALLOC(v.ws_c27, 27 * (NW > 0 ? NW : 1), int);
+  DALLOC(v.ws_o27, 27 * (NW > 0 ? NW : 1), int);
   DALLOC(v.lv_cnt[2], N, int);
   DALLOC(v.lv_off[2], N, int);
   DALLOC(v.dc, DC_SIZE, int);
@@ -1394,6 +1688,45 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   DALLOC(v.o_gc, 3 * N, double);
   DALLOC(v.o_gh, 3 * N, double);
   DALLOC(v.eatom, 7 * N, double);
+  DALLOC(v.acc_beta, N, double);
+  for (int k = 0; k < PA_NUM; k++) {
+    void *p;
+    if (dev_alloc(s, &p, sizeof(double) * (size_t)N)) return -1;
+    v.pa[k] = p;
+  }
+  {
+    /* pair-stage work list: tiles of ITILE atoms of one instance, each
+       split into nch partner chunks so that a single large instance still
+       gives every SM several blocks */
+    int ntiles = 0, maxn = 1;
+    for (int I = 0; I < NI; I++) {
+      int n = d->inst_begin[I + 1] - d->inst_begin[I];
+      ntiles += (n + ITILE - 1) / ITILE;
+      if (n > maxn) maxn = n;
+    }
+    int nch = (148 * 8 + ntiles - 1) / ntiles;
+    if (nch > maxn / 512) nch = maxn / 512;
+    if (nch < 1) nch = 1;
+    s->nch = nch;
+    s->nitems = ntiles * nch;
+    int4 *it = (int4 *)malloc(sizeof(int4) * s->nitems);
+    int q = 0;
+    for (int I = 0; I < NI; I++)
+      for (int a = d->inst_begin[I]; a < d->inst_begin[I + 1]; a += ITILE)
+        for (int c = 0; c < nch; c++) {
+          int e = a + ITILE < d->inst_begin[I + 1] ? a + ITILE : d->inst_begin[I + 1];
+          it[q].x = I;
+          it[q].y = a;
+          it[q].z = e;
+          it[q].w = c;
+          q++;
+        }
+    void *p;
+    if (dev_alloc(s, &p, sizeof(int4) * s->nitems)) return -1;
+    s->items = (int4 *)p;
+    if (upload(p, it, sizeof(int4) * s->nitems)) return -1;
+    free(it);
+  }
   DALLOC(v.ews, NW > 0 ? NW : 1, double);
   DALLOC(v.wsp, NW > 0 ? NW : 1, double);
   {
@@ -1412,6 +1745,8 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   dc0[DC_N] = N;
   dc0[DC_NB] = nb;
   dc0[DC_NWS] = NW;
+  dc0[DC_N27] = 27 * N;
+  dc0[DC_W27] = 27 * NW;
   if (upload(v.dc, dc0, sizeof(dc0))) return -1;
 
   /* capacities: kept overlaps per heavy atom at 0.05 atoms/A^3 are ~13,
@@ -1422,6 +1757,7 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   s->cap[3] = 64 * nheavy_tot + 4096;
   s->cap[4] = 64 * nheavy_tot + 4096;
   s->cap[5] = 32 * nheavy_tot + 4096;
+  s->cap_wsc = 64 * NW + 1024;
   /* AGBNP3_CAPACITY_SCALE (< 1) starts from smaller buffers, which
      exercises the overflow detection and regrowth of agb_dev_evaluate */
   const char *cs = getenv("AGBNP3_CAPACITY_SCALE");
@@ -1429,6 +1765,7 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     double f = atof(cs);
     s->cap_nl = (int)(s->cap_nl * f) + 1;
     for (int m = 2; m <= AGB_MAX_ORDER; m++) s->cap[m] = (int)(s->cap[m] * f) + 1;
+    s->cap_wsc = (int)(s->cap_wsc * f) + 1;
   }
   if (tree_alloc(s)) return -1;
   for (int k = 0; k <= AGB_NSTAGE; k++) CK(cudaEventCreate(&s->ev[k]));
@@ -1495,15 +1832,17 @@ static void launch_all(agb_dev *s) {
   cudaMemsetAsync(v.bucket_cursor, 0, sizeof(int) * v.nbuckets, st);
   cudaMemsetAsync(v.dc + DC_ERR, 0, sizeof(int), st);
   AGB_LAUNCH(k_prep, nblocks(N), BLK, st, v);
-  nl += 1;
+  AGB_LAUNCH(k_pack_geom<R>, nblocks(N), BLK, st, v);
+  nl += 2;
   stage_mark(s, 1);
   AGB_LAUNCH(k_cell_count, nblocks(N), BLK, st, v);
   agb_scan_excl(v.bucket_count, v.bucket_start, v.dc + DC_NB, v.dc + DC_C0 + 7, v.nbuckets, s->scan_scratch, st);
   AGB_LAUNCH(k_cell_fill, nblocks(N), BLK, st, v);
-  AGB_LAUNCH(k_nl_count, nblocks(N), BLK, st, v);
-  agb_scan_excl(v.nl_count, v.nl_off, v.dc + DC_N, v.dc + DC_NL, N, s->scan_scratch, st);
-  AGB_LAUNCH(k_nl_emit, nblocks(N), BLK, st, v);
-  nl += 4 + 6;
+  AGB_LAUNCH(k_nl_count27, nblocks(27LL * N), BLK, st, v);
+  agb_scan_excl(v.nl_c27, v.nl_o27, v.dc + DC_N27, v.dc + DC_NL, 27 * N, s->scan_scratch, st);
+  AGB_LAUNCH(k_nl_emit27, nblocks(27LL * N), BLK, st, v);
+  AGB_LAUNCH(k_nl_sort, nblocks(N), BLK, st, v);
+  nl += 5 + 6;
   stage_mark(s, 2);
   AGB_LAUNCH(k_l2_count<R>, nblocks(N), BLK, st, v);
   agb_scan_excl(v.lv_cnt[2], v.lv_off[2], v.dc + DC_N, v.dc + DC_L0 + 2, N, s->scan_scratch, st);
@@ -1518,21 +1857,29 @@ static void launch_all(agb_dev *s) {
   }
   stage_mark(s, 3);
   AGB_LAUNCH(k_scaling, nblocks(N), BLK, st, v);
-  nl += 1;
+  AGB_LAUNCH(k_pack_sp<R>, nblocks(N), BLK, st, v);
+  nl += 2;
   stage_mark(s, 4);
-  AGB_LAUNCH(k_descreen<R>, nblocks(N), BLK, st, v);
-  nl += 1;
+  int pgrid = s->nitems < 148 * 16 ? s->nitems : 148 * 16;
+  AGB_LAUNCH(k_descreen_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  AGB_LAUNCH(k_born<R>, nblocks(N), BLK, st, v);
+  nl += 2;
   stage_mark(s, 5);
-  AGB_LAUNCH(k_gbpair<R>, nblocks(N), BLK, st, v);
-  nl += 1;
+  AGB_LAUNCH(k_agb_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  AGB_LAUNCH(k_agb_post<R>, nblocks(N), BLK, st, v);
+  nl += 2;
   stage_mark(s, 6);
-  AGB_LAUNCH(k_gbders<R>, nblocks(N), BLK, st, v);
-  nl += 1;
+  AGB_LAUNCH(k_gbders_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  AGB_LAUNCH(k_gbders_post, nblocks(N), BLK, st, v);
+  nl += 2;
   stage_mark(s, 7);
   if (s->nws > 0) {
     AGB_LAUNCH(k_ws_geom<R>, nblocks(s->nws), BLK, st, v);
+    AGB_LAUNCH(k_ws_count27<R>, nblocks(27LL * s->nws), BLK, st, v);
+    agb_scan_excl(v.ws_c27, v.ws_o27, v.dc + DC_W27, v.dc + DC_WSC, 27 * s->nws, s->scan_scratch, st);
+    AGB_LAUNCH(k_ws_emit27<R>, nblocks(27LL * s->nws), BLK, st, v);
     AGB_LAUNCH(k_ws_free<R>, nblocks(s->nws), BLK, st, v);
-    nl += 2;
+    nl += 4 + 3;
   }
   stage_mark(s, 8);
   for (int m = 2; m <= AGB_MAX_ORDER; m++) {
@@ -1596,10 +1943,10 @@ extern "C" int agb_dev_evaluate(agb_dev *s) {
     s->last_stats[7] = dc[DC_ERR];
     s->last_stats[8] = s->nlaunch;
     int err = dc[DC_ERR];
-    if (err & AGB_ERR_WS_CAP) FAIL("more than %d heavy atoms within a water site's search radius", WS_MAXC);
-    if (err & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) {
+    if (err & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP | AGB_ERR_WS_CAP)) {
       /* grow what overflowed and evaluate again */
       if (dc[DC_NL] > s->cap_nl) s->cap_nl = 2 * dc[DC_NL];
+      if (dc[DC_WSC] > s->cap_wsc) s->cap_wsc = 2 * dc[DC_WSC];
       for (int m = 2; m <= AGB_MAX_ORDER; m++)
         if (dc[DC_L0 + m] > s->cap[m]) s->cap[m] = 2 * dc[DC_L0 + m];
       if (s->graph_ok) {

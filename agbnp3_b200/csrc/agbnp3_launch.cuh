@@ -15,6 +15,12 @@
 
 #define AGB_LAUNCH(kernel, grid, block, stream, ...) kernel<<<(grid), (block), 0, (stream)>>>(__VA_ARGS__)
 
+/* block-cooperative loop (each index handled by one thread of the block)
+   and the barrier that ends it */
+#define AGB_COOP_FOR(t, n) for (int t = threadIdx.x; t < (n); t += blockDim.x)
+#define AGB_SYNC() __syncthreads()
+#define AGB_SHARED __shared__
+
 #define AGB_GRID_STRIDE(i, n) \
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)(n); \
        i += (long long)gridDim.x * blockDim.x)

@@ -162,17 +162,21 @@ def test_batch_matches_members(engine):
 
 
 def test_caller_order_and_permutation(engine):
-    """Outputs follow the caller's atom order: a renumbered molecule gives
-    the same per-atom values, renumbered."""
+    """Outputs follow the caller's atom order.  AGBNP3 itself depends on
+    the atom numbering (the overlap tree is rooted at the lowest index and,
+    with Gaussian prefactors above 1, a larger overlap can exceed a smaller
+    one; the water-site order feeds the reference's free-volume index), so a
+    renumbered molecule is checked against the oracle of that numbering, and
+    its GB energy differs from the original only at the 1e-7 level."""
     s, _ = load_golden("globule300_shuffled")
     perm = np.random.default_rng(5).permutation(s.natoms)
-    a, b = A.Instance(s, precision=A.PREC_FP64), A.Instance(s.permuted(perm), precision=A.PREC_FP64)
+    sp = s.permuted(perm)
+    a, b = A.Instance(s, precision=A.PREC_FP64), A.Instance(sp, precision=A.PREC_FP64)
     try:
         Ra, Rb = a.ener(), b.ener()
-        for k in ENERGY_KEYS:
-            assert abs(Ra[k] - Rb[k]) <= 1e-9 * max(1.0, abs(Ra[k]))
-        for k in ("br", "sp", "dgbdr", "dehb"):
-            assert rms_rel(Rb[k], Ra[k][perm]) < 1e-9
+        check_vs_oracle(Rb, O.oracle_eval(sp), A.PREC_FP64, "permuted")
+        assert abs(Ra["egb"] - Rb["egb"]) <= 1e-6 * abs(Ra["egb"])
+        assert rms_rel(Rb["br"], Ra["br"][perm]) < 1e-5
     finally:
         a.close()
         b.close()
