@@ -77,6 +77,24 @@ void *agbnp3_batch_stream(int btag);
 int agbnp3_batch_stage_timing(int btag, int enable);
 int agbnp3_batch_stage_times(int btag, double *ms, int n);
 
+/* GB energy (self + pair, kcal/mol), its gradient at constant Born radii
+   (kcal/mol/A, [natoms][3]) and the A_i terms of the Born-radius chain rule,
+   for coordinates, charges and Born radii already on the device; all
+   arrays are device pointers and `stream` is a cudaStream_t (NULL: the
+   default stream).  It allocates no device memory: for callers that cannot
+   call cudaMalloc (an MD code that owns all device memory through its own
+   pool, work recorded into a CUDA graph, a plugin with a fixed memory
+   budget).  Its scratch is a static device array sized for at most 32768
+   atoms, held by every GPU that loads the library until exit; larger
+   systems are rejected with AGBNP_ERR.  The first call on each device
+   looks the array up with that device current and should come before any
+   stream capture.  Calls share the array, so calls that overlap on the GPU
+   race and must be serialised by the caller.  No counterpart in the
+   reference. */
+int agbnp3_gb_energy_static(int natoms, const double *x, const double *y, const double *z, const double *charge,
+                            const double *born_radii, double dielectric_in, double dielectric_out, double *egb,
+                            double *dera, double *dgbdr, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
