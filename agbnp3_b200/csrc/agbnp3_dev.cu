@@ -104,9 +104,12 @@ struct View {
   int nbuckets;
   void *pa[12];      /* packed pair-stage operands (R[natoms] each) */
   int *nl_c27, *nl_o27; /* near-list counts / offsets per (atom, neighbour cell) */
+  int *nl_tmp, *nl_own; /* unsorted entries and their atom */
   int *ws_c27, *ws_o27, *ws_cand; /* water-site candidates per (site, cell) */
   int cap_wsc;
   double *acc_beta; /* descreening sums */
+  const float *tab4_f;  /* [slot][k] = y_k, y2_k, y_k+1, y2_k+1 */
+  const double *tab4_d;
 };
 
 enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m */, DC_C0 = DC_L0 + 8 /* scratch */,
@@ -361,36 +364,39 @@ __global__ void k_nl_emit27(View v) {
              v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j) {
                float d2;
                if (j > g && near_test(a, v.pos[j], d2) && m < n) {
-                 v.nl_list[o + m] = j;
+                 v.nl_tmp[o + m] = j;
                  v.nl_d2[o + m] = d2;
+                 v.nl_own[o + m] = g;
                  m++;
                }
              });
   }
 }
 
-/* each atom's list in (float d^2, index) order (agbnp3.c:3766-3792,
-   4062-4066), and the per-atom CSR of the near list */
-__global__ void k_nl_sort(View v) {
+/* per-atom CSR of the near list */
+__global__ void k_nl_offsets(View v) {
   AGB_GRID_STRIDE(g, v.natoms) {
     int o = v.nl_o27[27 * g], e = (g + 1 < v.natoms) ? v.nl_o27[27 * (g + 1)] : v.dc[DC_NL];
     v.nl_off[g] = o;
     v.nl_count[g] = e - o;
-    if (e > v.cap_nl) continue;
-    int *lst = v.nl_list;
-    float *dd = v.nl_d2;
-    for (int a = o + 1; a < e; a++) {
-      int j = lst[a];
-      float d2 = dd[a];
-      int k = a;
-      while (k > o && (dd[k - 1] > d2 || (dd[k - 1] == d2 && lst[k - 1] > j))) {
-        dd[k] = dd[k - 1];
-        lst[k] = lst[k - 1];
-        k--;
-      }
-      dd[k] = d2;
-      lst[k] = j;
+  }
+}
+
+/* each atom's list in (float d^2, index) order (agbnp3.c:3766-3792,
+   4062-4066): one thread per entry places it at its rank */
+__global__ void k_nl_rank(View v) {
+  int n = min(v.dc[DC_NL], v.cap_nl);
+  AGB_GRID_STRIDE(e, n) {
+    if (v.dc[DC_ERR] & AGB_ERR_NL_CAP) continue;
+    int g = v.nl_own[e];
+    int o = v.nl_off[g], m = v.nl_count[g];
+    float d2 = v.nl_d2[e];
+    int j = v.nl_tmp[e], rank = 0;
+    for (int b = o; b < o + m; b++) {
+      float db = v.nl_d2[b];
+      rank += (db < d2) || (db == d2 && v.nl_tmp[b] < j);
     }
+    v.nl_list[o + rank] = j;
   }
 }
 
@@ -586,22 +592,6 @@ __device__ __forceinline__ R *pa(const View &v, int k) {
   return (R *)v.pa[k];
 }
 
-template <typename R>
-struct Vec2;
-template <>
-struct Vec2<float> {
-  typedef float2 T;
-};
-template <>
-struct Vec2<double> {
-  typedef double2 T;
-};
-
-template <typename R>
-__device__ __forceinline__ const typename Vec2<R>::T *tables2(const View &v) {
-  return (const typename Vec2<R>::T *)tables<R>(v);
-}
-
 /* exp(-d^2 / (4 Bi Bj)) as exp2 of a pre-scaled argument in float */
 template <typename R>
 struct GbExp;
@@ -617,20 +607,50 @@ struct GbExp<double> {
 };
 
 /* cubic spline of one Q4 table at xh = a / h in [0, AGB_NA-1): value and,
-   optionally, d/da (agbnp3_utils.c:229-252) */
+   optionally, d/da (agbnp3_utils.c:229-252).  The table holds one record
+   per interval, (y_k, y2_k, y_k+1, y2_k+1), so a lookup is one load. */
 template <typename R>
-__device__ __forceinline__ R spline(const typename Vec2<R>::T *tab, int slot, R xh, R &fp, bool want_fp,
+struct Rec4;
+template <>
+struct Rec4<float> {
+  typedef float4 T;
+  static __device__ __forceinline__ float4 ld(const float4 *p) { return __ldg(p); }
+};
+template <>
+struct Rec4<double> {
+  struct T {
+    double x, y, z, w;
+  };
+  static __device__ __forceinline__ T ld(const T *p) {
+    const double2 *q = (const double2 *)p;
+    double2 a = __ldg(q), b = __ldg(q + 1);
+    return T{a.x, a.y, b.x, b.y};
+  }
+};
+
+template <typename R>
+__device__ __forceinline__ const typename Rec4<R>::T *tables4(const View &v);
+template <>
+__device__ __forceinline__ const float4 *tables4<float>(const View &v) {
+  return (const float4 *)v.tab4_f;
+}
+template <>
+__device__ __forceinline__ const Rec4<double>::T *tables4<double>(const View &v) {
+  return (const Rec4<double>::T *)v.tab4_d;
+}
+
+template <typename R>
+__device__ __forceinline__ R spline(const typename Rec4<R>::T *tab, int slot, R xh, R &fp, bool want_fp,
                                     bool ref_sign) {
   const R h = R(C_AMAX / (AGB_NA - 1)), hinv = R((AGB_NA - 1) / C_AMAX);
   const R dp1 = h * R(1.0 / 6.0), dp2 = h * dp1;
   int k = (int)xh;
-  const typename Vec2<R>::T *t = tab + (size_t)slot * AGB_NA + k;
-  typename Vec2<R>::T t0 = __ldg(t), t1 = __ldg(t + 1);
+  typename Rec4<R>::T t = Rec4<R>::ld(tab + (size_t)slot * AGB_NA + k);
   R B = xh - R(k), A = R(1) - B;
-  R f = A * t0.x + B * t1.x + (A * (A * A - R(1)) * t0.y + B * (B * B - R(1)) * t1.y) * dp2;
+  R f = A * t.x + B * t.z + (A * (A * A - R(1)) * t.y + B * (B * B - R(1)) * t.w) * dp2;
   if (want_fp) {
-    R c1 = (R(3) * B * B - R(1)) * t1.y;
-    fp = (t1.x - t0.x) * hinv - ((R(3) * A * A - R(1)) * t0.y + (ref_sign ? c1 : -c1)) * dp1;
+    R c1 = (R(3) * B * B - R(1)) * t.w;
+    fp = (t.z - t.x) * hinv - ((R(3) * A * A - R(1)) * t.y + (ref_sign ? c1 : -c1)) * dp1;
   }
   return f;
 }
@@ -680,7 +700,7 @@ __global__ void __launch_bounds__(ITILE) k_descreen_t(View v, const int4 *__rest
   AGB_SHARED int st[ITILE];
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
   const R *RH = pa<R>(v, PA_RH), *W = pa<R>(v, PA_W);
-  const typename Vec2<R>::T *tab = tables2<R>(v);
+  const typename Rec4<R>::T *tab = tables4<R>(v);
   const int nt = v.ntypes;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     int4 w = items[it];
@@ -850,7 +870,7 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
   const R *RH = pa<R>(v, PA_RH), *RI = pa<R>(v, PA_RINV), *SP = pa<R>(v, PA_SP);
   const R *Q2 = pa<R>(v, PA_Q2AB), *AB = pa<R>(v, PA_ABRW);
-  const typename Vec2<R>::T *tab = tables2<R>(v);
+  const typename Rec4<R>::T *tab = tables4<R>(v);
   const int nt = v.ntypes;
   const bool rs = v.compat != 0;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -946,6 +966,238 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
       if (heavy) {
         atomicAdd(&v.deru[g], U);
         atomicAdd(&v.derv[g], V);
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* symmetric pair passes: each warp owns a 32-atom i tile and walks a run of */
+/* 32-atom j tiles (j >= i tile) of the same instance.  Lane l keeps atom i; */
+/* the j atoms' operands and their partial sums rotate through the warp with */
+/* __shfl_sync, so every unordered pair is evaluated exactly once and each j */
+/* atom's sums return to their lane after 32 rotations.  On a diagonal tile  */
+/* the rotations 1..16 cover each pair once (rotation 16 only on lanes < 16).*/
+/* Partial sums are float per tile pair, then double.                        */
+/* ------------------------------------------------------------------------ */
+#define FULLMASK 0xffffffffu
+
+template <typename T>
+__device__ __forceinline__ T rot1(T x) {
+  return __shfl_sync(FULLMASK, x, (threadIdx.x + 1) & 31);
+}
+
+/* agb: GB pair energy, constant-B gradient, A_i (agbnp3_cpu_simd_kernels.c:
+   66-151, 329-460) */
+template <typename R>
+__global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict__ items, int nitems) {
+  const int lane = threadIdx.x & 31;
+  const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
+  const R *Q = pa<R>(v, PA_Q), *Bv = pa<R>(v, PA_B), *BI = pa<R>(v, PA_BINV);
+  size_t N = v.natoms;
+  for (int it = blockIdx.x * 4 + (threadIdx.x >> 5); it < nitems; it += gridDim.x * 4) {
+    int4 w = items[it]; /* instance, first atom of the i tile, first atom of the j run, j tiles */
+    int a1 = v.inst_begin[w.x + 1];
+    int i = w.y + lane;
+    bool vi = i < a1;
+    R xi = vi ? X[i] : R(1e6), yi = vi ? Y[i] : R(0), zi = vi ? Z[i] : R(0);
+    R qi = vi ? Q[i] : R(0), bi = vi ? Bv[i] : R(1), ci = vi ? GbExp<R>::scale() * BI[i] : R(0);
+    double se = 0, sgx = 0, sgy = 0, sgz = 0, sat = 0;
+    for (int k = 0; k < w.w; k++) {
+      int j0 = w.z + 32 * k;
+      int j = j0 + lane;
+      bool vj = j < a1;
+      R xj = vj ? X[j] : R(-1e6), yj = vj ? Y[j] : R(0), zj = vj ? Z[j] : R(0);
+      R qj = vj ? Q[j] : R(0), bj = vj ? Bv[j] : R(1), bij = vj ? BI[j] : R(0);
+      R jgx = 0, jgy = 0, jgz = 0, jat = 0;
+      R pe = 0, pgx = 0, pgy = 0, pgz = 0, pat = 0;
+      const bool diag = j0 == w.y;
+      const int nrot = diag ? 16 : 32;
+      for (int r = diag ? 1 : 0; r <= nrot; r++) {
+        if (r > 0) {
+          xj = rot1(xj); yj = rot1(yj); zj = rot1(zj);
+          qj = rot1(qj); bj = rot1(bj); bij = rot1(bij);
+          jgx = rot1(jgx); jgy = rot1(jgy); jgz = rot1(jgz); jat = rot1(jat);
+        }
+        if (r == 32 || (diag && r == 16 && lane >= 16)) continue;
+        R dx = xj - xi, dy = yj - yi, dz = zj - zi;
+        R d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 > R(0)) || d2 > R(1e10)) continue; /* same / coincident / padding atoms */
+        R bb = bi * bj;
+        R et = GbExp<R>::ex(ci * bij * d2);
+        R f = m_rsqrt(d2 + bb * et);
+        R qq = qi * qj;
+        R qf3 = qq * f * f * f;
+        pe += qq * f;
+        R mw = (R(1) - R(0.25) * et) * qf3;
+        R gx = mw * dx, gy = mw * dy, gz = mw * dz;
+        pgx += gx; pgy += gy; pgz += gz;
+        jgx -= gx; jgy -= gy; jgz -= gz;
+        R at = (bb + R(0.25) * d2) * et * qf3;
+        pat += at;
+        jat += at;
+      }
+      if (diag) { /* 16 rotations: the j sums sit 16 lanes away */
+        int src = (lane + 16) & 31;
+        jgx = __shfl_sync(FULLMASK, jgx, src);
+        jgy = __shfl_sync(FULLMASK, jgy, src);
+        jgz = __shfl_sync(FULLMASK, jgz, src);
+        jat = __shfl_sync(FULLMASK, jat, src);
+      }
+      if (vj) {
+        double w2 = 2.0 * v.inst_df[w.x];
+        atomicAdd(&v.g_gb[3 * j], w2 * (double)jgx);
+        atomicAdd(&v.g_gb[3 * j + 1], w2 * (double)jgy);
+        atomicAdd(&v.g_gb[3 * j + 2], w2 * (double)jgz);
+        atomicAdd(&v.dera[j], (double)jat);
+      }
+      se += (double)pe;
+      sgx += (double)pgx;
+      sgy += (double)pgy;
+      sgz += (double)pgz;
+      sat += (double)pat;
+    }
+    if (vi) {
+      double w2 = 2.0 * v.inst_df[w.x];
+      atomicAdd(&v.eatom[N + i], C_TOKCAL * w2 * se);
+      atomicAdd(&v.g_gb[3 * i], w2 * sgx);
+      atomicAdd(&v.g_gb[3 * i + 1], w2 * sgy);
+      atomicAdd(&v.g_gb[3 * i + 2], w2 * sgz);
+      atomicAdd(&v.dera[i], sat);
+    }
+  }
+}
+
+/* gbders: both descreening directions of every unordered pair, pair forces,
+   U and V (agbnp3_cpu_simd_kernels.c:681-904); flags: bit 0 valid, bit 1
+   heavy */
+template <typename R>
+__global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restrict__ items, int nitems) {
+  const int lane = threadIdx.x & 31;
+  const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
+  const R *RH = pa<R>(v, PA_RH), *RI = pa<R>(v, PA_RINV), *SP = pa<R>(v, PA_SP);
+  const R *Q2 = pa<R>(v, PA_Q2AB), *AB = pa<R>(v, PA_ABRW);
+  const typename Rec4<R>::T *tab = tables4<R>(v);
+  const int nt = v.ntypes;
+  const bool rs = v.compat != 0;
+  for (int it = blockIdx.x * 4 + (threadIdx.x >> 5); it < nitems; it += gridDim.x * 4) {
+    int4 w = items[it];
+    int a0 = v.inst_begin[w.x], hh = a0 + v.inst_nheavy[w.x], a1 = v.inst_begin[w.x + 1];
+    int i = w.y + lane;
+    bool vi = i < a1, hi = i < hh;
+    R xi = vi ? X[i] : R(0), yi = vi ? Y[i] : R(0), zi = vi ? Z[i] : R(0);
+    R rhi = vi ? RH[i] : R(0), rii = vi ? RI[i] : R(0), spi = vi ? SP[i] : R(0);
+    R q2i = vi ? Q2[i] : R(0), abi = vi ? AB[i] : R(0);
+    int ti = vi ? v.rtype[i] : 0;
+    double sU = 0, sV = 0, sfx = 0, sfy = 0, sfz = 0, svx = 0, svy = 0, svz = 0;
+    for (int k = 0; k < w.w; k++) {
+      int j0 = w.z + 32 * k;
+      int j = j0 + lane;
+      bool vj = j < a1;
+      R xj = vj ? X[j] : R(0), yj = vj ? Y[j] : R(0), zj = vj ? Z[j] : R(0);
+      R rhj = vj ? RH[j] : R(0), rij = vj ? RI[j] : R(0), spj = vj ? SP[j] : R(0);
+      R q2j = vj ? Q2[j] : R(0), abj = vj ? AB[j] : R(0);
+      int fj = vj ? (v.rtype[j] << 2) | 1 | (j < hh ? 2 : 0) : 0;
+      R jU = 0, jV = 0, jfx = 0, jfy = 0, jfz = 0, jvx = 0, jvy = 0, jvz = 0;
+      R pU = 0, pV = 0, pfx = 0, pfy = 0, pfz = 0, pvx = 0, pvy = 0, pvz = 0;
+      const bool diag = j0 == w.y;
+      const int nrot = diag ? 16 : 32;
+      for (int r = diag ? 1 : 0; r <= nrot; r++) {
+        if (r > 0) {
+          xj = rot1(xj); yj = rot1(yj); zj = rot1(zj);
+          rhj = rot1(rhj); rij = rot1(rij); spj = rot1(spj);
+          q2j = rot1(q2j); abj = rot1(abj); fj = rot1(fj);
+          jU = rot1(jU); jV = rot1(jV);
+          jfx = rot1(jfx); jfy = rot1(jfy); jfz = rot1(jfz);
+          jvx = rot1(jvx); jvy = rot1(jvy); jvz = rot1(jvz);
+        }
+        if (r == 32 || (diag && r == 16 && lane >= 16)) continue;
+        bool hj = (fj & 2) != 0;
+        if (!vi || !(fj & 1) || !(hi || hj)) continue;
+        R dx = xj - xi, dy = yj - yi, dz = zj - zi;
+        R d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 > R(0))) continue;
+        R id = m_rsqrt(d2);
+        R d = d2 * id;
+        int tj = fj >> 2;
+        R ht = R(0), ut = R(0);
+        if (hi) { /* j descreened by i: table (type j, type i), radius of i */
+          R xh = d * rhi;
+          if (xh < R(AGB_NA - 1)) {
+            R fp;
+            R f = spline<R>(tab, tj * nt + ti, xh, fp, true, rs);
+            R q = f * rii, dq = fp * rii * rii;
+            pU += q2j * q;
+            pV += abj * q;
+            ht += q2j * dq * spi;
+            ut += abj * dq * spi;
+          }
+        }
+        if (hj) { /* i descreened by j: table (type i, type j), radius of j */
+          R xh = d * rhj;
+          if (xh < R(AGB_NA - 1)) {
+            R fp;
+            R f = spline<R>(tab, ti * nt + tj, xh, fp, true, rs);
+            R q = f * rij, dq = fp * rij * rij;
+            jU += q2i * q;
+            jV += abi * q;
+            ht += q2i * dq * spj;
+            ut += abi * dq * spj;
+          }
+        }
+        ht *= id;
+        ut *= id;
+        R fx = ht * dx, fy = ht * dy, fz = ht * dz;
+        R ux = ut * dx, uy = ut * dy, uz = ut * dz;
+        pfx += fx; pfy += fy; pfz += fz;
+        pvx += ux; pvy += uy; pvz += uz;
+        jfx -= fx; jfy -= fy; jfz -= fz;
+        jvx -= ux; jvy -= uy; jvz -= uz;
+      }
+      if (diag) {
+        int src = (lane + 16) & 31;
+        jU = __shfl_sync(FULLMASK, jU, src);
+        jV = __shfl_sync(FULLMASK, jV, src);
+        jfx = __shfl_sync(FULLMASK, jfx, src);
+        jfy = __shfl_sync(FULLMASK, jfy, src);
+        jfz = __shfl_sync(FULLMASK, jfz, src);
+        jvx = __shfl_sync(FULLMASK, jvx, src);
+        jvy = __shfl_sync(FULLMASK, jvy, src);
+        jvz = __shfl_sync(FULLMASK, jvz, src);
+      }
+      const double f4p = 1.0 / (4.0 * C_PI), kg = f4p * v.inst_df[w.x];
+      if (vj) {
+        atomicAdd(&v.g_gb[3 * j], kg * (double)jfx);
+        atomicAdd(&v.g_gb[3 * j + 1], kg * (double)jfy);
+        atomicAdd(&v.g_gb[3 * j + 2], kg * (double)jfz);
+        atomicAdd(&v.g_vw[3 * j], f4p * (double)jvx);
+        atomicAdd(&v.g_vw[3 * j + 1], f4p * (double)jvy);
+        atomicAdd(&v.g_vw[3 * j + 2], f4p * (double)jvz);
+        if (j < hh) {
+          atomicAdd(&v.deru[j], (double)jU);
+          atomicAdd(&v.derv[j], (double)jV);
+        }
+      }
+      sU += (double)pU;
+      sV += (double)pV;
+      sfx += (double)pfx;
+      sfy += (double)pfy;
+      sfz += (double)pfz;
+      svx += (double)pvx;
+      svy += (double)pvy;
+      svz += (double)pvz;
+    }
+    if (vi) {
+      const double f4p = 1.0 / (4.0 * C_PI), kg = f4p * v.inst_df[w.x];
+      atomicAdd(&v.g_gb[3 * i], kg * sfx);
+      atomicAdd(&v.g_gb[3 * i + 1], kg * sfy);
+      atomicAdd(&v.g_gb[3 * i + 2], kg * sfz);
+      atomicAdd(&v.g_vw[3 * i], f4p * svx);
+      atomicAdd(&v.g_vw[3 * i + 1], f4p * svy);
+      atomicAdd(&v.g_vw[3 * i + 2], f4p * svz);
+      if (hi) {
+        atomicAdd(&v.deru[i], sU);
+        atomicAdd(&v.derv[i], sV);
       }
     }
   }
@@ -1482,6 +1734,9 @@ struct agb_dev {
   long long last_stats[16];
   int4 *items; /* (instance, first atom, end atom, partner chunk) */
   int nitems, nch;
+  int4 *items_agb, *items_gbd; /* (instance, i tile, first j tile, j tiles) */
+  int n_agb, n_gbd;
+  int tiled_pairs; /* use the one-sided tiled pair kernels instead */
 };
 
 static int dev_alloc(agb_dev *s, void **p, size_t bytes) {
@@ -1524,6 +1779,9 @@ static int tree_free(agb_dev *s) {
   s->v.ws_cand = NULL;
   if (s->v.nl_list) cudaFree(s->v.nl_list);
   if (s->v.nl_d2) cudaFree(s->v.nl_d2);
+  if (s->v.nl_tmp) cudaFree(s->v.nl_tmp);
+  if (s->v.nl_own) cudaFree(s->v.nl_own);
+  s->v.nl_tmp = s->v.nl_own = NULL;
   if (s->scan_scratch) cudaFree(s->scan_scratch);
   s->v.nl_list = NULL;
   s->v.nl_d2 = NULL;
@@ -1537,6 +1795,8 @@ static int tree_alloc(agb_dev *s) {
   s->v.cap_wsc = s->cap_wsc;
   CK(cudaMalloc((void **)&s->v.nl_list, sizeof(int) * (size_t)s->cap_nl));
   CK(cudaMalloc((void **)&s->v.nl_d2, sizeof(float) * (size_t)s->cap_nl));
+  CK(cudaMalloc((void **)&s->v.nl_tmp, sizeof(int) * (size_t)s->cap_nl));
+  CK(cudaMalloc((void **)&s->v.nl_own, sizeof(int) * (size_t)s->cap_nl));
   int maxcap = s->natoms;
   for (int m = 2; m <= AGB_MAX_ORDER; m++) {
     CK(cudaMalloc((void **)&s->v.par[m], sizeof(int) * (size_t)m * s->cap[m]));
@@ -1636,6 +1896,27 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   UP(rtype, d->rtype, N, int);
   UP(tab_d, d->tab, ntab, double);
   UP(tab_f, tabf, ntab, float);
+  {
+    /* one record per interval: y_k, y2_k, y_k+1, y2_k+1 (the last node's
+       record is never read: a lookup stops below node AGB_NA-1) */
+    size_t nslot = (size_t)d->ntypes * d->ntypes;
+    double *t4 = (double *)calloc(nslot * AGB_NA * 4, sizeof(double));
+    float *t4f = (float *)calloc(nslot * AGB_NA * 4, sizeof(float));
+    for (size_t sl = 0; sl < nslot; sl++)
+      for (int k = 0; k + 1 < AGB_NA; k++) {
+        const double *a = d->tab + (sl * AGB_NA + k) * 2;
+        double *o = t4 + (sl * AGB_NA + k) * 4;
+        o[0] = a[0];
+        o[1] = a[1];
+        o[2] = a[2];
+        o[3] = a[3];
+        for (int c = 0; c < 4; c++) t4f[(sl * AGB_NA + k) * 4 + c] = (float)o[c];
+      }
+    UP(tab4_d, t4, nslot * AGB_NA * 4, double);
+    UP(tab4_f, t4f, nslot * AGB_NA * 4, float);
+    free(t4);
+    free(t4f);
+  }
   UP(ws_begin, d->ws_begin, NI + 1, int);
   if (NW > 0) {
     UP(ws_inst, ws_inst, NW, int);
@@ -1727,6 +2008,46 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     if (upload(p, it, sizeof(int4) * s->nitems)) return -1;
     free(it);
   }
+  {
+    /* symmetric passes: for every 32-atom i tile, runs of up to 8 j tiles
+       starting at the i tile; gbders skips i tiles of hydrogens only (their
+       j tiles are hydrogens too and hydrogens never descreen) */
+    const int JB = 8;
+    int cap = 0;
+    for (int I = 0; I < NI; I++) {
+      int T = (d->inst_begin[I + 1] - d->inst_begin[I] + 31) / 32;
+      cap += T * ((T + JB - 1) / JB);
+    }
+    int4 *ia = (int4 *)malloc(sizeof(int4) * (cap + 1)), *ig = (int4 *)malloc(sizeof(int4) * (cap + 1));
+    int na = 0, ng = 0;
+    for (int I = 0; I < NI; I++) {
+      int a0 = d->inst_begin[I], n = d->inst_begin[I + 1] - a0, T = (n + 31) / 32;
+      int hh = a0 + d->inst_nheavy[I];
+      for (int ti = 0; ti < T; ti++)
+        for (int tj = ti; tj < T; tj += JB) {
+          int4 q;
+          q.x = I;
+          q.y = a0 + 32 * ti;
+          q.z = a0 + 32 * tj;
+          q.w = (T - tj) < JB ? (T - tj) : JB;
+          ia[na++] = q;
+          if (q.y < hh) ig[ng++] = q;
+        }
+    }
+    void *p;
+    if (dev_alloc(s, &p, sizeof(int4) * (na + 1))) return -1;
+    s->items_agb = (int4 *)p;
+    if (upload(p, ia, sizeof(int4) * na)) return -1;
+    if (dev_alloc(s, &p, sizeof(int4) * (ng + 1))) return -1;
+    s->items_gbd = (int4 *)p;
+    if (upload(p, ig, sizeof(int4) * ng)) return -1;
+    s->n_agb = na;
+    s->n_gbd = ng;
+    free(ia);
+    free(ig);
+    const char *tp = getenv("AGBNP3_PAIR_TILED");
+    s->tiled_pairs = tp && atoi(tp) != 0;
+  }
   DALLOC(v.ews, NW > 0 ? NW : 1, double);
   DALLOC(v.wsp, NW > 0 ? NW : 1, double);
   {
@@ -1816,6 +2137,13 @@ static inline int nblocks(long long n) {
   return (int)b;
 }
 
+/* blocks of 4 warps, one work item per warp */
+static inline int sym_grid(int n) {
+  int b = (n + 3) / 4;
+  if (b > 148 * 16) b = 148 * 16;
+  return b < 1 ? 1 : b;
+}
+
 static void stage_mark(agb_dev *s, int k) {
   if (s->timing) cudaEventRecord(s->ev[k], s->st);
 }
@@ -1841,8 +2169,9 @@ static void launch_all(agb_dev *s) {
   AGB_LAUNCH(k_nl_count27, nblocks(27LL * N), BLK, st, v);
   agb_scan_excl(v.nl_c27, v.nl_o27, v.dc + DC_N27, v.dc + DC_NL, 27 * N, s->scan_scratch, st);
   AGB_LAUNCH(k_nl_emit27, nblocks(27LL * N), BLK, st, v);
-  AGB_LAUNCH(k_nl_sort, nblocks(N), BLK, st, v);
-  nl += 5 + 6;
+  AGB_LAUNCH(k_nl_offsets, nblocks(N), BLK, st, v);
+  AGB_LAUNCH(k_nl_rank, nblocks(s->cap_nl), BLK, st, v);
+  nl += 6 + 6;
   stage_mark(s, 2);
   AGB_LAUNCH(k_l2_count<R>, nblocks(N), BLK, st, v);
   agb_scan_excl(v.lv_cnt[2], v.lv_off[2], v.dc + DC_N, v.dc + DC_L0 + 2, N, s->scan_scratch, st);
@@ -1865,11 +2194,17 @@ static void launch_all(agb_dev *s) {
   AGB_LAUNCH(k_born<R>, nblocks(N), BLK, st, v);
   nl += 2;
   stage_mark(s, 5);
-  AGB_LAUNCH(k_agb_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  if (s->tiled_pairs)
+    AGB_LAUNCH(k_agb_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  else
+    AGB_LAUNCH(k_agb_sym<R>, sym_grid(s->n_agb), 128, st, v, s->items_agb, s->n_agb);
   AGB_LAUNCH(k_agb_post<R>, nblocks(N), BLK, st, v);
   nl += 2;
   stage_mark(s, 6);
-  AGB_LAUNCH(k_gbders_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  if (s->tiled_pairs)
+    AGB_LAUNCH(k_gbders_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  else
+    AGB_LAUNCH(k_gbders_sym<R>, sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
   AGB_LAUNCH(k_gbders_post, nblocks(N), BLK, st, v);
   nl += 2;
   stage_mark(s, 7);
