@@ -89,6 +89,8 @@ def lib():
         L.agbnp3_batch_stream.restype = _vp
         L.agbnp3_batch_stage_timing.argtypes = [ctypes.c_int, ctypes.c_int]
         L.agbnp3_batch_stage_times.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
+        L.agbnp3_autotune.argtypes = [ctypes.c_int, _ip, ctypes.c_int]
+        L.agbnp3_batch_autotune.argtypes = [ctypes.c_int, _ip, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -263,6 +265,13 @@ class Instance:
         a, _ = self.debug_fetch(100 + k, self.natoms, np.float64)
         return a[: self.natoms]
 
+    def autotune(self) -> dict:
+        """Times the pair-stage work decompositions at the current device
+        coordinates and keeps the fastest (agbnp3_autotune)."""
+        p = np.zeros(4, np.int32)
+        _check(lib().agbnp3_autotune(self.tag, _p(p, _ip), 4), "agbnp3_autotune")
+        return dict(desc_chunks=int(p[0]), sym_run=int(p[1]), invb_us=int(p[2]), pair_us=int(p[3]))
+
     def close(self):
         if self.tag is not None:
             delete(self.tag)
@@ -319,6 +328,11 @@ class Batch:
         ms = np.zeros(16)
         n = lib().agbnp3_batch_stage_times(self.btag, _p(ms), 16)
         return {lib().agbnp3_stage_name(k).decode(): float(ms[k]) for k in range(n)}
+
+    def autotune(self) -> dict:
+        p = np.zeros(4, np.int32)
+        _check(lib().agbnp3_batch_autotune(self.btag, _p(p, _ip), 4), "agbnp3_batch_autotune")
+        return dict(desc_chunks=int(p[0]), sym_run=int(p[1]), invb_us=int(p[2]), pair_us=int(p[3]))
 
     def close(self):
         if self.btag is not None:

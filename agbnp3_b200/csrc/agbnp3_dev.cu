@@ -1737,6 +1737,8 @@ struct agb_dev {
   int4 *items_agb, *items_gbd; /* (instance, i tile, first j tile, j tiles) */
   int n_agb, n_gbd;
   int tiled_pairs; /* use the one-sided tiled pair kernels instead */
+  int jb;          /* j tiles per symmetric work item */
+  int *h_inst_nheavy;
 };
 
 static int dev_alloc(agb_dev *s, void **p, size_t bytes) {
@@ -1819,6 +1821,86 @@ static int tree_alloc(agb_dev *s) {
   return 0;
 }
 
+/* pair-stage work lists.  One-sided passes (invb and the tiled fallback):
+   tiles of ITILE atoms of one instance, each split into nch partner chunks
+   (nch = 0: enough chunks for ~8 blocks per SM).  Symmetric passes: for
+   every 32-atom i tile, runs of up to jb j tiles starting at the i tile;
+   gbders skips i tiles of hydrogens only (their j tiles are hydrogens too
+   and hydrogens never descreen). */
+static int build_items(agb_dev *s, int nch, int jb) {
+  int NI = s->ninst;
+  const int *ib = s->h_inst_begin, *inh = s->h_inst_nheavy;
+  int ntiles = 0, maxn = 1;
+  for (int I = 0; I < NI; I++) {
+    int n = ib[I + 1] - ib[I];
+    ntiles += (n + ITILE - 1) / ITILE;
+    if (n > maxn) maxn = n;
+  }
+  if (nch <= 0) {
+    nch = (148 * 8 + ntiles - 1) / ntiles;
+    if (nch > maxn / 512) nch = maxn / 512;
+  }
+  if (nch < 1) nch = 1;
+  if (jb < 1) jb = 1;
+  s->nch = nch;
+  s->jb = jb;
+  int nit = ntiles * nch;
+  int4 *it = (int4 *)malloc(sizeof(int4) * nit);
+  int q = 0;
+  for (int I = 0; I < NI; I++)
+    for (int a = ib[I]; a < ib[I + 1]; a += ITILE)
+      for (int c = 0; c < nch; c++) {
+        int e = a + ITILE < ib[I + 1] ? a + ITILE : ib[I + 1];
+        it[q].x = I;
+        it[q].y = a;
+        it[q].z = e;
+        it[q].w = c;
+        q++;
+      }
+  int cap = 0;
+  for (int I = 0; I < NI; I++) {
+    int T = (ib[I + 1] - ib[I] + 31) / 32;
+    cap += T * ((T + jb - 1) / jb);
+  }
+  int4 *ia = (int4 *)malloc(sizeof(int4) * (cap + 1)), *ig = (int4 *)malloc(sizeof(int4) * (cap + 1));
+  int na = 0, ng = 0;
+  for (int I = 0; I < NI; I++) {
+    int a0 = ib[I], n = ib[I + 1] - a0, T = (n + 31) / 32;
+    int hh = a0 + inh[I];
+    for (int ti = 0; ti < T; ti++)
+      for (int tj = ti; tj < T; tj += jb) {
+        int4 w;
+        w.x = I;
+        w.y = a0 + 32 * ti;
+        w.z = a0 + 32 * tj;
+        w.w = (T - tj) < jb ? (T - tj) : jb;
+        ia[na++] = w;
+        if (w.y < hh) ig[ng++] = w;
+      }
+  }
+  if (s->items) cudaFree(s->items);
+  if (s->items_agb) cudaFree(s->items_agb);
+  if (s->items_gbd) cudaFree(s->items_gbd);
+  s->items = s->items_agb = s->items_gbd = NULL;
+  CK(cudaMalloc((void **)&s->items, sizeof(int4) * nit));
+  CK(cudaMalloc((void **)&s->items_agb, sizeof(int4) * (na + 1)));
+  CK(cudaMalloc((void **)&s->items_gbd, sizeof(int4) * (ng + 1)));
+  CK(cudaMemcpy(s->items, it, sizeof(int4) * nit, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->items_agb, ia, sizeof(int4) * na, cudaMemcpyHostToDevice));
+  if (ng) CK(cudaMemcpy(s->items_gbd, ig, sizeof(int4) * ng, cudaMemcpyHostToDevice));
+  s->nitems = nit;
+  s->n_agb = na;
+  s->n_gbd = ng;
+  free(it);
+  free(ia);
+  free(ig);
+  if (s->graph_ok) {
+    cudaGraphExecDestroy(s->gexec);
+    s->graph_ok = 0;
+  }
+  return 0;
+}
+
 extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   *out = NULL;
   if (d->natoms <= 0 || d->ninst <= 0) FAIL("empty system");
@@ -1846,6 +1928,8 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   s->h_ws_begin = (int *)malloc(sizeof(int) * (NI + 1));
   memcpy(s->h_inst_begin, d->inst_begin, sizeof(int) * (NI + 1));
   memcpy(s->h_ws_begin, d->ws_begin, sizeof(int) * (NI + 1));
+  s->h_inst_nheavy = (int *)malloc(sizeof(int) * NI);
+  memcpy(s->h_inst_nheavy, d->inst_nheavy, sizeof(int) * NI);
 
   /* static per-instance data */
   int *inst_of = (int *)malloc(sizeof(int) * N);
@@ -1976,78 +2060,15 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     v.pa[k] = p;
   }
   {
-    /* pair-stage work list: tiles of ITILE atoms of one instance, each
-       split into nch partner chunks so that a single large instance still
-       gives every SM several blocks */
-    int ntiles = 0, maxn = 1;
-    for (int I = 0; I < NI; I++) {
-      int n = d->inst_begin[I + 1] - d->inst_begin[I];
-      ntiles += (n + ITILE - 1) / ITILE;
-      if (n > maxn) maxn = n;
-    }
-    int nch = (148 * 8 + ntiles - 1) / ntiles;
-    if (nch > maxn / 512) nch = maxn / 512;
-    if (nch < 1) nch = 1;
-    s->nch = nch;
-    s->nitems = ntiles * nch;
-    int4 *it = (int4 *)malloc(sizeof(int4) * s->nitems);
-    int q = 0;
-    for (int I = 0; I < NI; I++)
-      for (int a = d->inst_begin[I]; a < d->inst_begin[I + 1]; a += ITILE)
-        for (int c = 0; c < nch; c++) {
-          int e = a + ITILE < d->inst_begin[I + 1] ? a + ITILE : d->inst_begin[I + 1];
-          it[q].x = I;
-          it[q].y = a;
-          it[q].z = e;
-          it[q].w = c;
-          q++;
-        }
-    void *p;
-    if (dev_alloc(s, &p, sizeof(int4) * s->nitems)) return -1;
-    s->items = (int4 *)p;
-    if (upload(p, it, sizeof(int4) * s->nitems)) return -1;
-    free(it);
-  }
-  {
-    /* symmetric passes: for every 32-atom i tile, runs of up to 8 j tiles
-       starting at the i tile; gbders skips i tiles of hydrogens only (their
-       j tiles are hydrogens too and hydrogens never descreen) */
-    const int JB = 8;
-    int cap = 0;
-    for (int I = 0; I < NI; I++) {
-      int T = (d->inst_begin[I + 1] - d->inst_begin[I] + 31) / 32;
-      cap += T * ((T + JB - 1) / JB);
-    }
-    int4 *ia = (int4 *)malloc(sizeof(int4) * (cap + 1)), *ig = (int4 *)malloc(sizeof(int4) * (cap + 1));
-    int na = 0, ng = 0;
-    for (int I = 0; I < NI; I++) {
-      int a0 = d->inst_begin[I], n = d->inst_begin[I + 1] - a0, T = (n + 31) / 32;
-      int hh = a0 + d->inst_nheavy[I];
-      for (int ti = 0; ti < T; ti++)
-        for (int tj = ti; tj < T; tj += JB) {
-          int4 q;
-          q.x = I;
-          q.y = a0 + 32 * ti;
-          q.z = a0 + 32 * tj;
-          q.w = (T - tj) < JB ? (T - tj) : JB;
-          ia[na++] = q;
-          if (q.y < hh) ig[ng++] = q;
-        }
-    }
-    void *p;
-    if (dev_alloc(s, &p, sizeof(int4) * (na + 1))) return -1;
-    s->items_agb = (int4 *)p;
-    if (upload(p, ia, sizeof(int4) * na)) return -1;
-    if (dev_alloc(s, &p, sizeof(int4) * (ng + 1))) return -1;
-    s->items_gbd = (int4 *)p;
-    if (upload(p, ig, sizeof(int4) * ng)) return -1;
-    s->n_agb = na;
-    s->n_gbd = ng;
-    free(ia);
-    free(ig);
     const char *tp = getenv("AGBNP3_PAIR_TILED");
     s->tiled_pairs = tp && atoi(tp) != 0;
+    int nch = 0, jb = 8;
+    const char *e1 = getenv("AGBNP3_DESC_CHUNKS"), *e2 = getenv("AGBNP3_SYM_RUN");
+    if (e1) nch = atoi(e1);
+    if (e2) jb = atoi(e2);
+    if (build_items(s, nch, jb)) return -1;
   }
+
   DALLOC(v.ews, NW > 0 ? NW : 1, double);
   DALLOC(v.wsp, NW > 0 ? NW : 1, double);
   {
@@ -2104,8 +2125,12 @@ extern "C" void agb_dev_destroy(agb_dev *s) {
   for (int k = 0; k <= AGB_NSTAGE; k++)
     if (s->ev[k]) cudaEventDestroy(s->ev[k]);
   cudaStreamDestroy(s->st);
+  if (s->items) cudaFree(s->items);
+  if (s->items_agb) cudaFree(s->items_agb);
+  if (s->items_gbd) cudaFree(s->items_gbd);
   free(s->h_inst_begin);
   free(s->h_ws_begin);
+  free(s->h_inst_nheavy);
   free(s);
 }
 
@@ -2396,3 +2421,72 @@ extern "C" long long agb_dev_debug_fetch(agb_dev *s, int what, void *out, long l
   }
   return -1;
 }
+
+/* Autotuner for the pair-stage decomposition: tries partner-chunk counts
+   for the one-sided descreening pass and j-run lengths for the symmetric
+   passes on the current coordinates (stage timers, median of `reps`
+   evaluations after one warm-up), keeps the fastest and returns
+   params = {nch, jb, invb_us, agb_gbders_us}.  With params_in set, applies
+   them without timing. */
+extern "C" int agb_dev_autotune(agb_dev *s, int reps, const int *params_in, int *params_out) {
+  CK(cudaSetDevice(s->device));
+  if (params_in) {
+    if (build_items(s, params_in[0], params_in[1])) return -1;
+    if (params_out) {
+      params_out[0] = s->nch;
+      params_out[1] = s->jb;
+      params_out[2] = params_out[3] = -1;
+    }
+    return 0;
+  }
+  if (reps < 1) reps = 1;
+  int timing = s->timing;
+  s->timing = 1;
+  int maxh = 1;
+  for (int I = 0; I < s->ninst; I++)
+    if (s->h_inst_nheavy[I] > maxh) maxh = s->h_inst_nheavy[I];
+  const int nchs[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32};
+  const int jbs[] = {2, 4, 8, 16, 32};
+  double best = 1e30;
+  int bn = 1, bj = s->jb;
+  double samp[16];
+  for (size_t a = 0; a < sizeof(nchs) / sizeof(nchs[0]); a++) {
+    if (nchs[a] > 1 && maxh / nchs[a] < 128) break;
+    if (build_items(s, nchs[a], bj)) return -1;
+    for (int r = 0; r <= reps; r++) {
+      if (agb_dev_evaluate(s)) return -1;
+      if (r) samp[r - 1] = s->stage_ms[4];
+    }
+    double m = samp[0];
+    for (int r = 1; r < reps; r++) m = samp[r] < m ? samp[r] : m;
+    if (m < best) {
+      best = m;
+      bn = nchs[a];
+    }
+  }
+  double tinvb = best;
+  best = 1e30;
+  for (size_t a = 0; a < sizeof(jbs) / sizeof(jbs[0]); a++) {
+    if (build_items(s, bn, jbs[a])) return -1;
+    for (int r = 0; r <= reps; r++) {
+      if (agb_dev_evaluate(s)) return -1;
+      if (r) samp[r - 1] = s->stage_ms[5] + s->stage_ms[6];
+    }
+    double m = samp[0];
+    for (int r = 1; r < reps; r++) m = samp[r] < m ? samp[r] : m;
+    if (m < best) {
+      best = m;
+      bj = jbs[a];
+    }
+  }
+  if (build_items(s, bn, bj)) return -1;
+  s->timing = timing;
+  if (params_out) {
+    params_out[0] = bn;
+    params_out[1] = bj;
+    params_out[2] = (int)(1e3 * tinvb);
+    params_out[3] = (int)(1e3 * best);
+  }
+  return 0;
+}
+

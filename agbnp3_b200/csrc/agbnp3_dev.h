@@ -101,6 +101,10 @@ const char *agb_dev_stage_name(int i);
    overlaps of orders 2..5, [5] candidate overlaps, [6] water sites,
    [7] device error word, [8] kernels launched per evaluation */
 int agb_dev_stats(agb_dev *s, long long *out, int n);
+/* tunes the pair-stage work decomposition on the current coordinates
+   (params_in NULL) or applies params_in = {nch, jb}; params_out = {nch, jb,
+   invb us, agb+gbders us} */
+int agb_dev_autotune(agb_dev *s, int reps, const int *params_in, int *params_out);
 /* copies internal arrays of the last evaluation for parity tests */
 long long agb_dev_debug_fetch(agb_dev *s, int what, void *out, long long cap);
 

@@ -938,3 +938,69 @@ int agbnp3_batch_stage_times(int btag, double *ms, int n) {
   batch_t *B = get_batch(btag, "agbnp3_batch_stage_times()");
   return B ? agb_dev_stage_times(B->dev, ms, n) : AGBNP_ERR;
 }
+
+/* ------------------------------------------------------------------ */
+/* autotuner with an optional cache file ($AGBNP3_TUNE_CACHE): one line */
+/* per key "<instances>:<size bucket> <nch> <jb>"                       */
+/* ------------------------------------------------------------------ */
+static void tune_key(char *key, size_t n, int ninst, int natoms) {
+  int bucket = (int)floor(4.0 * log2((double)natoms > 1 ? (double)natoms : 1.0));
+  snprintf(key, n, "%d:%d", ninst, bucket);
+}
+
+static int tune_lookup(const char *key, int *p) {
+  const char *path = getenv("AGBNP3_TUNE_CACHE");
+  if (!path) return 0;
+  FILE *f = fopen(path, "r");
+  if (!f) return 0;
+  char k[64];
+  int a, b, found = 0;
+  while (fscanf(f, "%63s %d %d", k, &a, &b) == 3)
+    if (strcmp(k, key) == 0) {
+      p[0] = a;
+      p[1] = b;
+      found = 1;
+    }
+  fclose(f);
+  return found;
+}
+
+static void tune_store(const char *key, const int *p) {
+  const char *path = getenv("AGBNP3_TUNE_CACHE");
+  if (!path) return;
+  FILE *f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "%s %d %d\n", key, p[0], p[1]);
+  fclose(f);
+}
+
+static int autotune_dev(agb_dev *dev, int ninst, int natoms, int *params, int n, const char *who) {
+  char key[64];
+  int p[4] = {0, 0, -1, -1}, rc;
+  tune_key(key, sizeof(key), ninst, natoms);
+  if (tune_lookup(key, p))
+    rc = agb_dev_autotune(dev, 0, p, p);
+  else {
+    rc = agb_dev_autotune(dev, 3, NULL, p);
+    if (rc == 0) tune_store(key, p);
+  }
+  if (rc != 0) {
+    errprint("%s: %s", who, agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  for (int k = 0; k < n && k < 4; k++) params[k] = p[k];
+  return AGBNP_OK;
+}
+
+int agbnp3_autotune(int tag, int *params, int n) {
+  inst_t *I = get_inst(tag, "agbnp3_autotune()");
+  if (!I) return AGBNP_ERR;
+  return autotune_dev(I->dev, 1, I->natoms, params, n, "agbnp3_autotune()");
+}
+
+int agbnp3_batch_autotune(int btag, int *params, int n) {
+  batch_t *B = get_batch(btag, "agbnp3_batch_autotune()");
+  if (!B) return AGBNP_ERR;
+  return autotune_dev(B->dev, B->n, B->natoms, params, n, "agbnp3_batch_autotune()");
+}
+

@@ -42,6 +42,10 @@ def parse():
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--fp64-steps", type=int, default=5)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--config", default="globule25k", choices=["globule25k", "batch512"],
+                   help="globule25k: one 25,000-atom globule (headline); batch512: 512 instances of "
+                        "300-5,000 atoms (log-uniform) with 0.2 A coordinate noise, one batched evaluation per step")
+    p.add_argument("--ninst", type=int, default=512)
     return p.parse_args()
 
 
@@ -154,6 +158,86 @@ def reference_arm(args):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def batch_systems(A, ninst, seed, rank=0):
+    from agbnp3_b200.shard import rank_seed
+    rs = rank_seed(seed, 1000 * rank)
+    rng = np.random.default_rng(rs)
+    sizes = np.exp(rng.uniform(np.log(300), np.log(5000), ninst)).astype(int)
+    return [A.make_globule(int(n), rs * 100003 + k, noise=0.2) for k, n in enumerate(sizes)]
+
+
+def batch_main(args, A, torch, rank, world, local):
+    """512 independent instances (log-uniform 300-5,000 atoms, 0.2 A noise)
+    evaluated together: one step = one batched evaluation of all instances;
+    the metric is instance evaluations per second."""
+    systems = batch_systems(A, args.ninst, args.seed, rank)
+    insts = [A.Instance(x, precision=A.PREC_MIXED) for x in systems]
+    B = A.Batch(insts)
+    B.set_mode(A.PREC_MIXED, True)
+    xyz = np.concatenate([x.coords() for x in systems])
+    B.set_coords(xyz)
+    B.ener_resident()
+    tune = B.autotune()
+    stream = torch.cuda.ExternalStream(B.stream, device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        B.ener_resident()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            B.ener_resident()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    from agbnp3_b200.shard import max_over_ranks, throughput
+    tot = max_over_ranks(sum(times), world, f"cuda:{local}")
+    value = throughput(args.ninst * args.steps, tot / 1e3, world)
+    B.stage_timing(True)
+    B.ener_resident()
+    stage_ms = B.stage_times()
+    B.stage_timing(False)
+    # e2e: host coordinates in, all outputs out, every step
+    e2e = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        B.set_coords(xyz)
+        B.ener_resident()
+        B.results()
+        e2e.append(time.perf_counter() - t0)
+    R = B.results()
+    # accuracy of the batched mixed path against the FP64 path on 8 members
+    acc = []
+    for k in range(0, args.ninst, max(1, args.ninst // 8)):
+        a = A.Instance(systems[k], precision=A.PREC_FP64)
+        F = a.ener()
+        e_m = sum(R[q][k] for q in ("egb", "evdw", "ecav", "ehb"))
+        e_f = sum(F[q] for q in ("egb", "evdw", "ecav", "ehb"))
+        acc.append(abs(e_m - e_f) / abs(e_f))
+        a.close()
+    if rank == 0:
+        natoms = int(sum(x.natoms for x in systems))
+        print(json.dumps({
+            "metric": "instance energy+grad evals/s, 512-instance batch (300-5,000 atoms)", "value": value,
+            "unit": "evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tot / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 math / f64 accumulation", "data": "synthetic",
+            "config": {"workload": f"batch of {args.ninst} globules, {natoms} atoms total, 0.2 A noise",
+                       "l2": "256 MB flush between timed steps", "autotune": tune},
+            "stage_ms": stage_ms,
+            "e2e": {"value": world * args.ninst * args.steps / sum(e2e), "unit": "evals/s",
+                    "h2d_bytes_per_step": 3 * 8 * natoms, "d2h_bytes_per_step": 15 * 8 * natoms + 56 * args.ninst},
+            "accuracy_vs_fp64": {"max_energy_rel_err": max(acc)},
+            "clocks": clk.summary()}))
+    B.close()
+    for i in insts:
+        i.close()
+
+
 # ----------------------------------------------------------------------------
 # engine arm
 # ----------------------------------------------------------------------------
@@ -172,9 +256,16 @@ def main():
     import agbnp3_b200 as A
     A.lib().agbnp3_set_device(local)
     A.initialize()
+    if args.config == "batch512":
+        batch_main(args, A, torch, rank, world, local)
+        A.terminate()
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
 
+    from agbnp3_b200.shard import max_over_ranks, rank_seed, throughput
     natoms = args.natoms
-    s = A.make_globule(natoms, args.seed + rank)
+    s = A.make_globule(natoms, rank_seed(args.seed, rank))
     inst = A.Instance(s, precision=A.PREC_MIXED, compat=True)
     ref_out = inst.ener()  # sizes the buffers, captures the graph
     stream = torch.cuda.ExternalStream(inst.stream, device=torch.device("cuda", local))
@@ -206,12 +297,8 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    tot_ms = sum(times)
-    if world > 1:
-        t = torch.tensor([tot_ms], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = world * args.steps / (tot_ms / 1e3)
+    tot_ms = max_over_ranks(sum(times), world, f"cuda:{local}")
+    value = throughput(args.steps, tot_ms / 1e3, world)
     mixed = inst.results()
     st = inst.stats()
 
@@ -229,7 +316,7 @@ def main():
     inst64 = A.Instance(s, precision=A.PREC_FP64, compat=True)
     inst64.ener()
     t64 = timed_resident(inst64, args.fp64_steps, 1)
-    fp64_value = world * len(t64) / (sum(t64) / 1e3)
+    fp64_value = throughput(len(t64), max_over_ranks(sum(t64), world, f"cuda:{local}") / 1e3, world)
     full = inst64.results()
     inst64.close()
     tot = lambda R: sum(R[k] for k in ("egb", "evdw", "ecav", "ehb"))  # noqa: E731
@@ -267,12 +354,8 @@ def main():
         t0 = time.perf_counter()
         call()
         e2e_t.append(time.perf_counter() - t0)
-    e2e_tot = sum(e2e_t)
-    if world > 1:
-        t = torch.tensor([e2e_tot], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_tot = float(t.item())
-    e2e_value = world * args.steps / e2e_tot
+    e2e_tot = max_over_ranks(sum(e2e_t), world, f"cuda:{local}")
+    e2e_value = throughput(args.steps, e2e_tot, world)
 
     # dominant stage and its arithmetic rate (pair counts x
     # frozen per-pair operation weights)

@@ -58,6 +58,15 @@ int agbnp3_stats(int tag, long long *out, int n);
    agbnp3_dev.cu, DBG_*); returns the element count or a negative value */
 long long agbnp3_debug_fetch(int tag, int what, void *out, long long cap);
 
+/* autotuner: times the pair-stage work decompositions (partner chunks of
+   the descreening pass, j-tile runs of the symmetric passes) on the
+   current coordinates and keeps the fastest; with $AGBNP3_TUNE_CACHE set,
+   choices are read from / appended to that file, keyed by instance count
+   and size bucket.  params (n <= 4): nch, jb, descreening us, pair passes us
+   (-1 when taken from the cache) */
+int agbnp3_autotune(int tag, int *params, int n);
+int agbnp3_batch_autotune(int btag, int *params, int n);
+
 /* message of the last error */
 const char *agbnp3_last_error(void);
 
