@@ -436,20 +436,17 @@ __device__ __forceinline__ void rec_put(const View &v, int m, int q, const Ov<R>
 }
 
 /* self-volume and surface-area contributions of one kept overlap of order
-   m with parents par[] (agbnp3_cpu_simd_kernels.c:1322-1345) */
-template <typename R>
-__device__ __forceinline__ void add_volumes(const View &v, int m, const int *par, const Ov<R> &o) {
-  double coef = ((m & 1) ? 1.0 : -1.0) / m; /* (-1)^(m+1) / m */
-  R sgn = (m & 1) ? R(1) : R(-1);           /* m * coef */
+   M to its parent k (agbnp3_cpu_simd_kernels.c:1322-1345) */
+template <typename R, int M>
+__device__ __forceinline__ void vol_terms(const View &v, int k, const Ov<R> &o, double &dvol, double &dsurf) {
+  const double coef = ((M & 1) ? 1.0 : -1.0) / M; /* (-1)^(M+1) / M */
+  const R sgn = (M & 1) ? R(1) : R(-1);           /* M * coef */
   R h3 = sgn * o.fp * R(3) / o.a, h4 = R(0.5) * sgn * o.fp;
-  for (int ii = 0; ii < m; ii++) {
-    int k = par[ii];
-    atomicAdd(&v.volumep[k], coef * (double)o.gvolp);
-    R u1 = atom_alpha<R>(v, k) * o.gvol, u2 = R(-2) * u1;
-    R v0 = u2 * (px<R>(v, k) - o.cx), v1 = u2 * (py<R>(v, k) - o.cy), v2 = u2 * (pz<R>(v, k) - o.cz);
-    R d2 = v0 * v0 + v1 * v1 + v2 * v2;
-    atomicAdd(&v.surf[k], (double)((h3 * u1 + h4 * d2 / u1) / (R)v.r[k]));
-  }
+  R u1 = atom_alpha<R>(v, k) * o.gvol, u2 = R(-2) * u1;
+  R v0 = u2 * (px<R>(v, k) - o.cx), v1 = u2 * (py<R>(v, k) - o.cy), v2 = u2 * (pz<R>(v, k) - o.cz);
+  R d2 = v0 * v0 + v1 * v1 + v2 * v2;
+  dvol = coef * (double)o.gvolp;
+  dsurf = (double)((h3 * u1 + h4 * d2 / u1) / (R)v.r[k]);
 }
 
 /* order 2: candidates are the near-list pairs of each heavy atom */
@@ -467,6 +464,8 @@ __global__ void k_l2_count(View v) {
   }
 }
 
+/* the records of one thread share their first parent: its sums stay in
+   registers and go out with one atomic each at the end */
 template <typename R>
 __global__ void k_l2_emit(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
@@ -474,72 +473,103 @@ __global__ void k_l2_emit(View v) {
     int n = v.nl_count[g], o = v.nl_off[g];
     if (n == 0 || o + n > v.cap_nl) continue;
     int q = v.lv_off[2][g], qend = q + v.lv_cnt[2][g];
+    if (q == qend) continue;
     if (qend > v.cap[2]) {
       set_err(v, AGB_ERR_TREE_CAP);
       continue;
     }
+    double svol = 0.0, ssurf = 0.0;
     for (int k = 0; k < n; k++) {
       int j = v.nl_list[o + k];
       Ov<R> ov = atom_pair<R>(v, (int)g, j);
       if (!kept(ov.gvolp)) continue;
-      int par[2] = {(int)g, j};
-      v.par[2][q] = par[0];
-      v.par[2][v.cap[2] + q] = par[1];
+      v.par[2][q] = (int)g;
+      v.par[2][v.cap[2] + q] = j;
       rec_put<R>(v, 2, q, ov);
       v.gend[2][q] = qend;
-      add_volumes<R>(v, 2, par, ov);
+      double dv, ds;
+      vol_terms<R, 2>(v, (int)g, ov, dv, ds);
+      svol += dv;
+      ssurf += ds;
+      vol_terms<R, 2>(v, j, ov, dv, ds);
+      atomicAdd(&v.volumep[j], dv);
+      atomicAdd(&v.surf[j], ds);
       q++;
     }
+    atomicAdd(&v.volumep[g], svol);
+    atomicAdd(&v.surf[g], ssurf);
   }
 }
 
-/* order m >= 3: overlap a combines with the last atom of every later
+/* order M >= 3: overlap a combines with the last atom of every later
    overlap b of its group (same generating overlap one order down) */
-template <typename R>
-__global__ void k_lm_count(View v, int m) {
+template <typename R, int M>
+__global__ void k_lm_count(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
-  int n = min(v.dc[DC_L0 + m - 1], v.cap[m - 1]);
-  int cm = v.cap[m - 1];
+  const int n = min(v.dc[DC_L0 + M - 1], v.cap[M - 1]);
+  const int cm = v.cap[M - 1];
   AGB_GRID_STRIDE(a, n) {
-    int ge = v.gend[m - 1][a], cnt = 0;
-    R aa = rec_get<R>(v, m - 1, a, F_A), ap = rec_get<R>(v, m - 1, a, F_P);
-    R ax = rec_get<R>(v, m - 1, a, F_CX), ay = rec_get<R>(v, m - 1, a, F_CY), az = rec_get<R>(v, m - 1, a, F_CZ);
+    int ge = v.gend[M - 1][a], cnt = 0;
+    R aa = rec_get<R>(v, M - 1, a, F_A), ap = rec_get<R>(v, M - 1, a, F_P);
+    R ax = rec_get<R>(v, M - 1, a, F_CX), ay = rec_get<R>(v, M - 1, a, F_CY), az = rec_get<R>(v, M - 1, a, F_CZ);
     for (int b = a + 1; b < ge; b++) {
-      int j = v.par[m - 1][(size_t)(m - 2) * cm + b];
+      int j = v.par[M - 1][(size_t)(M - 2) * cm + b];
       Ov<R> ov = ogauss<R>(aa, ap, ax, ay, az, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j), pz<R>(v, j));
       if (kept(ov.gvolp)) cnt++;
     }
-    v.lv_cnt[m][a] = cnt;
+    v.lv_cnt[M][a] = cnt;
   }
 }
 
-template <typename R>
-__global__ void k_lm_emit(View v, int m) {
+/* the records of one thread share parents 0..M-2: their sums stay in
+   registers and go out with one atomic each at the end */
+template <typename R, int M>
+__global__ void k_lm_emit(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
-  int n = min(v.dc[DC_L0 + m - 1], v.cap[m - 1]);
-  int cm = v.cap[m - 1], cn = v.cap[m];
+  const int n = min(v.dc[DC_L0 + M - 1], v.cap[M - 1]);
+  const int cm = v.cap[M - 1], cn = v.cap[M];
   AGB_GRID_STRIDE(a, n) {
-    int q = v.lv_off[m][a], qend = q + v.lv_cnt[m][a];
+    int q = v.lv_off[M][a], qend = q + v.lv_cnt[M][a];
     if (q == qend) continue;
     if (qend > cn) {
       set_err(v, AGB_ERR_TREE_CAP);
       continue;
     }
-    int ge = v.gend[m - 1][a];
-    int par[AGB_MAX_ORDER];
-    for (int k = 0; k < m - 1; k++) par[k] = v.par[m - 1][(size_t)k * cm + a];
-    R aa = rec_get<R>(v, m - 1, a, F_A), ap = rec_get<R>(v, m - 1, a, F_P);
-    R ax = rec_get<R>(v, m - 1, a, F_CX), ay = rec_get<R>(v, m - 1, a, F_CY), az = rec_get<R>(v, m - 1, a, F_CZ);
+    int ge = v.gend[M - 1][a];
+    int par[M - 1];
+    double svol[M - 1], ssurf[M - 1];
+#pragma unroll
+    for (int k = 0; k < M - 1; k++) {
+      par[k] = v.par[M - 1][(size_t)k * cm + a];
+      svol[k] = ssurf[k] = 0.0;
+    }
+    R aa = rec_get<R>(v, M - 1, a, F_A), ap = rec_get<R>(v, M - 1, a, F_P);
+    R ax = rec_get<R>(v, M - 1, a, F_CX), ay = rec_get<R>(v, M - 1, a, F_CY), az = rec_get<R>(v, M - 1, a, F_CZ);
     for (int b = a + 1; b < ge; b++) {
-      int j = v.par[m - 1][(size_t)(m - 2) * cm + b];
+      int j = v.par[M - 1][(size_t)(M - 2) * cm + b];
       Ov<R> ov = ogauss<R>(aa, ap, ax, ay, az, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j), pz<R>(v, j));
       if (!kept(ov.gvolp)) continue;
-      par[m - 1] = j;
-      for (int k = 0; k < m; k++) v.par[m][(size_t)k * cn + q] = par[k];
-      rec_put<R>(v, m, q, ov);
-      v.gend[m][q] = qend;
-      add_volumes<R>(v, m, par, ov);
+#pragma unroll
+      for (int k = 0; k < M - 1; k++) v.par[M][(size_t)k * cn + q] = par[k];
+      v.par[M][(size_t)(M - 1) * cn + q] = j;
+      rec_put<R>(v, M, q, ov);
+      v.gend[M][q] = qend;
+      double dv, ds;
+#pragma unroll
+      for (int k = 0; k < M - 1; k++) {
+        vol_terms<R, M>(v, par[k], ov, dv, ds);
+        svol[k] += dv;
+        ssurf[k] += ds;
+      }
+      vol_terms<R, M>(v, j, ov, dv, ds);
+      atomicAdd(&v.volumep[j], dv);
+      atomicAdd(&v.surf[j], ds);
       q++;
+    }
+#pragma unroll
+    for (int k = 0; k < M - 1; k++) {
+      atomicAdd(&v.volumep[par[k]], svol[k]);
+      atomicAdd(&v.surf[par[k]], ssurf[k]);
     }
   }
 }
@@ -1565,84 +1595,129 @@ __global__ void k_ws_free(View v) {
 /* ------------------------------------------------------------------------ */
 /* treeders: derivatives through the self volumes and surface areas         */
 /* ------------------------------------------------------------------------ */
-template <typename R>
-__global__ void k_tree_ders(View v, int m) {
+/* inclusive sum of a[] over the run of consecutive lanes holding this
+   lane's key (a key may come back in a later run, which is summed apart);
+   returns whether this lane ends its run */
+__device__ __forceinline__ bool seg_scan12(double (&a)[12], int key) {
+  const int lane = threadIdx.x & 31;
+  int kp = __shfl_up_sync(0xffffffffu, key, 1);
+  int kn = __shfl_down_sync(0xffffffffu, key, 1);
+  unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || kp != key);
+  int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane))); /* last head at or before this lane */
+  for (int o = 1; o < 32; o <<= 1) {
+    bool take = lane - o >= start;
+#pragma unroll
+    for (int c = 0; c < 12; c++) {
+      double t = __shfl_up_sync(0xffffffffu, a[c], o);
+      if (take) a[c] += t;
+    }
+  }
+  return lane == 31 || kn != key;
+}
+
+template <typename R, int M>
+__global__ void __launch_bounds__(256) k_tree_ders(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
-  int n = min(v.dc[DC_L0 + m], v.cap[m]);
-  int cm = v.cap[m];
+  const int n = min(v.dc[DC_L0 + M], v.cap[M]);
+  const int cm = v.cap[M];
   const double f4p = 1.0 / (4.0 * C_PI);
-  double coef = ((m & 1) ? 1.0 : -1.0) / m;
-  double sgn = (m & 1) ? 1.0 : -1.0;
-  AGB_GRID_STRIDE(q, n) {
-    int par[AGB_MAX_ORDER];
-    for (int k = 0; k < m; k++) par[k] = v.par[m][(size_t)k * cm + q];
-    R cx = rec_get<R>(v, m, q, F_CX), cy = rec_get<R>(v, m, q, F_CY), cz = rec_get<R>(v, m, q, F_CZ);
-    R gvol = rec_get<R>(v, m, q, F_GVOL), fp = rec_get<R>(v, m, q, F_FP), fpp = rec_get<R>(v, m, q, F_FPP);
-    R inva = R(1) / rec_get<R>(v, m, q, F_A);
-    int I = v.inst_of[par[0]];
-    double df = v.inst_df[I];
+  const double coef = ((M & 1) ? 1.0 : -1.0) / M;
+  const double sgn = (M & 1) ? 1.0 : -1.0;
+  const int lane = threadIdx.x & 31;
+  /* warp-uniform loop: 32 consecutive records per warp step, so that runs of
+     records sharing a parent are reduced in the warp before the atomics */
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long base = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n;
+       base += nwarps * 32) {
+    const int q = (int)base + lane;
+    const bool act = q < n;
+    int par[M];
+    R gdr[M][3], gdR[M], ga[M], gr[M];
+    double wc[M], wv[M], wb[M];
     double su = 0, sv = 0, sh = 0;
-    for (int k = 0; k < m; k++) {
-      su += v.deru[par[k]];
-      sv += v.derv[par[k]];
-      sh += v.derh[par[k]];
+    R fp = R(0), h3 = R(0), inva = R(0);
+#pragma unroll
+    for (int k = 0; k < M; k++) {
+      par[k] = act ? v.par[M][(size_t)k * cm + q] : 0;
+      gdr[k][0] = gdr[k][1] = gdr[k][2] = R(0);
+      gdR[k] = ga[k] = R(0);
+      gr[k] = R(1);
+      wc[k] = wv[k] = wb[k] = 0.0;
     }
-    su *= -df * f4p * coef;
-    sv *= -f4p * coef;
-    sh *= -coef;
-    R gdr[AGB_MAX_ORDER][3], gdR[AGB_MAX_ORDER], ga[AGB_MAX_ORDER], gr[AGB_MAX_ORDER];
-    double acc[AGB_MAX_ORDER][4][3]; /* gb, vw, hb, cav per parent */
-    for (int ii = 0; ii < m; ii++) {
-      int k = par[ii];
-      ga[ii] = atom_alpha<R>(v, k);
-      gr[ii] = (R)v.r[k];
-      R u1 = ga[ii] * gvol;
-      R xk[3] = {px<R>(v, k) - cx, py<R>(v, k) - cy, pz<R>(v, k) - cz};
-      R d2 = R(0);
-      for (int c = 0; c < 3; c++) {
-        gdr[ii][c] = R(-2) * u1 * xk[c];
-        d2 += gdr[ii][c] * gdr[ii][c];
-        double ur = (double)(gdr[ii][c] * fp); /* -2 u1 fp (x - c) */
-        acc[ii][0][c] = su * ur;
-        acc[ii][1][c] = sv * ur;
-        acc[ii][2][c] = sh * ur;
-        acc[ii][3][c] = 0.0;
+    if (act) {
+      R cx = rec_get<R>(v, M, q, F_CX), cy = rec_get<R>(v, M, q, F_CY), cz = rec_get<R>(v, M, q, F_CZ);
+      R gvol = rec_get<R>(v, M, q, F_GVOL), fpp = rec_get<R>(v, M, q, F_FPP);
+      fp = rec_get<R>(v, M, q, F_FP);
+      inva = R(1) / rec_get<R>(v, M, q, F_A);
+      double df = v.inst_df[v.inst_of[par[0]]];
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        int a = par[k];
+        su += v.deru[a];
+        sv += v.derv[a];
+        sh += v.derh[a];
+        wc[k] = sgn * v.gammap[a];
+        wv[k] = sgn * v.dervs[a];
+        wb[k] = sgn * v.derus[a];
+        ga[k] = atom_alpha<R>(v, a);
+        gr[k] = (R)v.r[a];
+        R u1 = ga[k] * gvol;
+        R xk[3] = {px<R>(v, a) - cx, py<R>(v, a) - cy, pz<R>(v, a) - cz};
+        R d2 = R(0);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          gdr[k][c] = R(-2) * u1 * xk[c];
+          d2 += gdr[k][c] * gdr[k][c];
+        }
+        gdR[k] = (R(3) * inva * u1 + R(0.5) * d2 / u1) / gr[k];
       }
-      gdR[ii] = (R(3) * inva * u1 + R(0.5) * d2 / u1) / gr[ii];
+      su *= -df * f4p * coef;
+      sv *= -f4p * coef;
+      sh *= -coef;
+      h3 = fpp + fp / gvol;
     }
-    R h3 = fpp + fp / gvol;
-    for (int ii = 0; ii < m; ii++) { /* diagonal terms */
-      int k = par[ii];
-      R u1 = R(-2) * fp * (R(1) - ga[ii] * inva) / gr[ii] + h3 * gdR[ii];
-      double wc = sgn * v.gammap[k], wv = sgn * v.dervs[k], wb = sgn * v.derus[k];
+    const R h4 = R(2) * fp * inva;
+#pragma unroll
+    for (int ii = 0; ii < M; ii++) {
+      /* gradient on parent ii: gb xyz, vdw xyz, hb xyz, cavity xyz */
+      double acc[12];
+      R ud = R(-2) * fp * (R(1) - ga[ii] * inva) / gr[ii] + h3 * gdR[ii];
+#pragma unroll
       for (int c = 0; c < 3; c++) {
-        double ur = (double)(u1 * gdr[ii][c]);
-        acc[ii][3][c] += wc * ur;
-        acc[ii][1][c] += wv * ur;
-        acc[ii][0][c] += wb * ur;
+        double ur = (double)(gdr[ii][c] * fp);
+        double dd = (double)(ud * gdr[ii][c]);
+        acc[c] = su * ur + wb[ii] * dd;
+        acc[3 + c] = sv * ur + wv[ii] * dd;
+        acc[6 + c] = sh * ur;
+        acc[9 + c] = wc[ii] * dd;
       }
-    }
-    R h4 = R(2) * fp * inva;
-    for (int ii = 0; ii < m; ii++) /* off-diagonal terms */
-      for (int jj = 0; jj < m; jj++) {
+#pragma unroll
+      for (int jj = 0; jj < M; jj++) {
         if (jj == ii) continue;
-        int l = par[jj];
         R u1 = h4 * ga[ii] / gr[jj], u2 = h3 * gdR[jj];
-        double wc = sgn * v.gammap[l], wv = sgn * v.dervs[l], wb = sgn * v.derus[l];
+#pragma unroll
         for (int c = 0; c < 3; c++) {
           double ur = (double)(u1 * gdr[jj][c] + u2 * gdr[ii][c]);
-          acc[ii][3][c] += wc * ur;
-          acc[ii][1][c] += wv * ur;
-          acc[ii][0][c] += wb * ur;
+          acc[9 + c] += wc[jj] * ur;
+          acc[3 + c] += wv[jj] * ur;
+          acc[c] += wb[jj] * ur;
         }
       }
-    for (int ii = 0; ii < m; ii++) {
-      int k = par[ii];
-      for (int c = 0; c < 3; c++) {
-        atomicAdd(&v.g_gb[3 * k + c], acc[ii][0][c]);
-        atomicAdd(&v.g_vw[3 * k + c], acc[ii][1][c]);
-        atomicAdd(&v.g_hb[3 * k + c], acc[ii][2][c]);
-        atomicAdd(&v.g_cav[3 * k + c], acc[ii][3][c]);
+      /* parents 0..M-2 are shared by runs of consecutive records (records
+         are stored in tree order): sum each run in the warp and let its last
+         lane do one atomic per component; the last parent differs from
+         record to record */
+      int key = act ? par[ii] : -1 - lane;
+      bool tail = true;
+      if (ii < M - 1) tail = seg_scan12(acc, key);
+      if (act && tail) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          atomicAdd(&v.g_gb[3 * key + c], acc[c]);
+          atomicAdd(&v.g_vw[3 * key + c], acc[3 + c]);
+          atomicAdd(&v.g_hb[3 * key + c], acc[6 + c]);
+          atomicAdd(&v.g_cav[3 * key + c], acc[9 + c]);
+        }
       }
     }
   }
@@ -2203,10 +2278,19 @@ static void launch_all(agb_dev *s) {
   AGB_LAUNCH(k_l2_emit<R>, nblocks(N), BLK, st, v);
   nl += 2 + 3;
   for (int m = 3; m <= AGB_MAX_ORDER; m++) {
-    AGB_LAUNCH(k_lm_count<R>, nblocks(v.cap[m - 1]), BLK, st, v, m);
+    int g = nblocks(v.cap[m - 1]);
+    switch (m) {
+      case 3: AGB_LAUNCH((k_lm_count<R, 3>), g, BLK, st, v); break;
+      case 4: AGB_LAUNCH((k_lm_count<R, 4>), g, BLK, st, v); break;
+      default: AGB_LAUNCH((k_lm_count<R, 5>), g, BLK, st, v); break;
+    }
     agb_scan_excl(v.lv_cnt[m], v.lv_off[m], v.dc + DC_L0 + m - 1, v.dc + DC_L0 + m, v.cap[m - 1], s->scan_scratch,
                   st);
-    AGB_LAUNCH(k_lm_emit<R>, nblocks(v.cap[m - 1]), BLK, st, v, m);
+    switch (m) {
+      case 3: AGB_LAUNCH((k_lm_emit<R, 3>), g, BLK, st, v); break;
+      case 4: AGB_LAUNCH((k_lm_emit<R, 4>), g, BLK, st, v); break;
+      default: AGB_LAUNCH((k_lm_emit<R, 5>), g, BLK, st, v); break;
+    }
     nl += 2 + 3;
   }
   stage_mark(s, 3);
@@ -2243,7 +2327,12 @@ static void launch_all(agb_dev *s) {
   }
   stage_mark(s, 8);
   for (int m = 2; m <= AGB_MAX_ORDER; m++) {
-    AGB_LAUNCH(k_tree_ders<R>, nblocks(v.cap[m]), BLK, st, v, m);
+    switch (m) {
+      case 2: AGB_LAUNCH((k_tree_ders<R, 2>), nblocks(v.cap[m]), BLK, st, v); break;
+      case 3: AGB_LAUNCH((k_tree_ders<R, 3>), nblocks(v.cap[m]), BLK, st, v); break;
+      case 4: AGB_LAUNCH((k_tree_ders<R, 4>), nblocks(v.cap[m]), BLK, st, v); break;
+      default: AGB_LAUNCH((k_tree_ders<R, 5>), nblocks(v.cap[m]), BLK, st, v); break;
+    }
     nl += 1;
   }
   stage_mark(s, 9);

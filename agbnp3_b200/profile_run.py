@@ -1,6 +1,6 @@
 """Runs a fixed number of evaluations of one workload, for profilers.
 
-    python -m agbnp3_b200.profile_run --natoms 25000 --evals 3 --mode mixed
+    python -m agbnp3_b200.profile_run --natoms 25000 --evals 3 --mode mixed [--autotune]
     python -m agbnp3_b200.profile_run --batch 64 --evals 2
 
 The first evaluation sizes the buffers and captures the CUDA graph; the
@@ -22,6 +22,7 @@ def main():
     p.add_argument("--mode", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--batch", type=int, default=0, help="instances of log-uniform size in [300, 5000]")
     p.add_argument("--timing", action="store_true", help="print per-stage device times")
+    p.add_argument("--autotune", action="store_true", help="tune the pair-stage decomposition first")
     a = p.parse_args()
     prec = A.PREC_MIXED if a.mode == "mixed" else A.PREC_FP64
     A.initialize()
@@ -38,6 +39,8 @@ def main():
         obj = A.Instance(s, precision=prec)
         obj.set_coords(s.coords())
         natoms = s.natoms
+    if a.autotune:
+        print("autotune:", obj.autotune())
     obj.stage_timing(a.timing)
     t = time.perf_counter()
     for _ in range(a.evals):
