@@ -75,8 +75,6 @@ struct View {
   const int *ext_of;
   const double *r, *charge, *igamma, *sgamma, *ialpha, *salpha, *vols;
   const int *rtype;
-  const double *tab_d;
-  const float *tab_f;
   const int *ws_kind, *ws_parent, *ws_nparent, *ws_prev;
   const double *ws_khb;
   /* per evaluation */
@@ -108,8 +106,9 @@ struct View {
   int *ws_c27, *ws_o27, *ws_cand; /* water-site candidates per (site, cell) */
   int cap_wsc;
   double *acc_beta; /* descreening sums */
-  const float *tab4_f;  /* [slot][k] = y_k, y2_k, y_k+1, y2_k+1 */
-  const double *tab4_d;
+  /* Q4 tables as per-interval cubics in t = a/h - k, c0..c3 */
+  const float4 *tabv_f;
+  const double4 *tabv_d;
 };
 
 enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m */, DC_C0 = DC_L0 + 8 /* scratch */,
@@ -147,13 +146,6 @@ template <>
 __device__ __forceinline__ float pz<float>(const View &v, int g) { return v.pos[g].z; }
 template <>
 __device__ __forceinline__ double pz<double>(const View &v, int g) { return v.pzd[g]; }
-
-template <typename R>
-__device__ __forceinline__ const R *tables(const View &v);
-template <>
-__device__ __forceinline__ const float *tables<float>(const View &v) { return v.tab_f; }
-template <>
-__device__ __forceinline__ const double *tables<double>(const View &v) { return v.tab_d; }
 
 __device__ __forceinline__ void set_err(const View &v, int bit) { atomicOr(&v.dc[DC_ERR], bit); }
 
@@ -207,36 +199,6 @@ __device__ __forceinline__ Ov<R> ogauss(R a1, R p1, R x1, R y1, R z1, R a2, R p2
 template <typename R>
 __device__ __forceinline__ bool kept(R gvolp) {
   return gvolp > R(FLT_MIN);
-}
-
-/* Q4 of an atom (radius type td) descreened by a heavy atom of type ts and
-   radius Rs at distance d, and dQ4/dd; cubic-spline lookup at a = d/Rs
-   (agbnp3_utils.c:229-252, 297-377).  `ref_sign` keeps the reference's
-   sign of the second curvature term of the derivative (agbnp3_utils.c:
-   250-251). */
-template <typename R>
-__device__ __forceinline__ R q4(const R *tab, int ntypes, int td, int ts, R d, R Rs, R &dq, bool want_dq,
-                                bool ref_sign) {
-  const R h = R(C_AMAX / (AGB_NA - 1));
-  const R hinv = R((AGB_NA - 1) / C_AMAX);
-  R rinv = R(1) / Rs;
-  R xh = d * rinv * hinv;
-  if (!(xh >= R(0)) || !(xh < R(AGB_NA - 1))) { /* beyond a = 20 (or NaN): Q4 = 0 */
-    dq = R(0);
-    return R(0);
-  }
-  int k = (int)xh;
-  const R *t = tab + ((size_t)(td * ntypes + ts) * AGB_NA + k) * 2;
-  R y0 = t[0], c0 = t[1], y1 = t[2], c1 = t[3];
-  R A = R(k + 1) - xh, B = xh - R(k);
-  R dp1 = h * R(1.0 / 6.0), dp2 = h * dp1;
-  R f = A * y0 + B * y1 + ((A * A * A - A) * c0 + (B * B * B - B) * c1) * dp2;
-  if (want_dq) {
-    R s2 = ref_sign ? R(1) : R(-1);
-    R fp = (y1 - y0) * hinv - ((R(3) * A * A - R(1)) * c0 + s2 * (R(3) * B * B - R(1)) * c1) * dp1;
-    dq = fp * rinv * rinv;
-  }
-  return f * rinv;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -636,53 +598,55 @@ struct GbExp<double> {
   static __device__ __forceinline__ double ex(double a) { return exp(a); }
 };
 
-/* cubic spline of one Q4 table at xh = a / h in [0, AGB_NA-1): value and,
-   optionally, d/da (agbnp3_utils.c:229-252).  The table holds one record
-   per interval, (y_k, y2_k, y_k+1, y2_k+1), so a lookup is one load. */
+/* cubic spline of one Q4 table at xh = a / h in [0, AGB_NA-1)
+   (agbnp3_utils.c:229-252), stored per interval k as the cubic in
+   t = xh - k, f = c0 + t (c1 + t (c2 + t c3)), one 16-byte (float) or
+   32-byte (double) record per lookup.  The spline's second derivatives at
+   the interval ends are y2_k = 2 c2 / h^2 and y2_k+1 = (6 c3 + 2 c2) / h^2,
+   so the record also gives d/da:
+     exact:      (c1 + 2 c2 t + 3 c3 t^2) / h
+     reference:  the exact one minus (3 t^2 - 1) h y2_k+1 / 3
+                 (agbnp3_utils.c:247-249 adds the y2_k+1 curvature term
+                 where the spline derivative subtracts it)
+   i.e. (c1 + k(2 c3 + 2 c2 / 3) + 2 c2 t + (3 c3 - k(6 c3 + 2 c2)) t^2) / h
+   with k = 1 for the reference's sign, 0 for the exact derivative. */
 template <typename R>
-struct Rec4;
+struct Tab;
 template <>
-struct Rec4<float> {
+struct Tab<float> {
   typedef float4 T;
   static __device__ __forceinline__ float4 ld(const float4 *p) { return __ldg(p); }
+  static __device__ __forceinline__ const float4 *val(const View &v) { return v.tabv_f; }
 };
 template <>
-struct Rec4<double> {
-  struct T {
-    double x, y, z, w;
-  };
-  static __device__ __forceinline__ T ld(const T *p) {
+struct Tab<double> {
+  typedef double4 T;
+  static __device__ __forceinline__ double4 ld(const double4 *p) {
     const double2 *q = (const double2 *)p;
     double2 a = __ldg(q), b = __ldg(q + 1);
-    return T{a.x, a.y, b.x, b.y};
+    return make_double4(a.x, a.y, b.x, b.y);
   }
+  static __device__ __forceinline__ const double4 *val(const View &v) { return v.tabv_d; }
 };
 
 template <typename R>
-__device__ __forceinline__ const typename Rec4<R>::T *tables4(const View &v);
-template <>
-__device__ __forceinline__ const float4 *tables4<float>(const View &v) {
-  return (const float4 *)v.tab4_f;
-}
-template <>
-__device__ __forceinline__ const Rec4<double>::T *tables4<double>(const View &v) {
-  return (const Rec4<double>::T *)v.tab4_d;
+__device__ __forceinline__ R spline(const typename Tab<R>::T *tv, int slot, R xh) {
+  int k = (int)xh;
+  R t = xh - R(k);
+  typename Tab<R>::T c = Tab<R>::ld(tv + (size_t)slot * AGB_NA + k);
+  return c.x + t * (c.y + t * (c.z + t * c.w));
 }
 
+/* value and h * d/da; kref = 1 for the reference's derivative, 0 exact */
 template <typename R>
-__device__ __forceinline__ R spline(const typename Rec4<R>::T *tab, int slot, R xh, R &fp, bool want_fp,
-                                    bool ref_sign) {
-  const R h = R(C_AMAX / (AGB_NA - 1)), hinv = R((AGB_NA - 1) / C_AMAX);
-  const R dp1 = h * R(1.0 / 6.0), dp2 = h * dp1;
+__device__ __forceinline__ R spline_d(const typename Tab<R>::T *tv, int slot, R xh, R kref, R &fph) {
   int k = (int)xh;
-  typename Rec4<R>::T t = Rec4<R>::ld(tab + (size_t)slot * AGB_NA + k);
-  R B = xh - R(k), A = R(1) - B;
-  R f = A * t.x + B * t.z + (A * (A * A - R(1)) * t.y + B * (B * B - R(1)) * t.w) * dp2;
-  if (want_fp) {
-    R c1 = (R(3) * B * B - R(1)) * t.w;
-    fp = (t.z - t.x) * hinv - ((R(3) * A * A - R(1)) * t.y + (ref_sign ? c1 : -c1)) * dp1;
-  }
-  return f;
+  R t = xh - R(k);
+  typename Tab<R>::T c = Tab<R>::ld(tv + (size_t)slot * AGB_NA + k);
+  R d0 = c.y + kref * (R(2) * c.w + R(2.0 / 3.0) * c.z);
+  R d2 = R(3) * c.w - kref * (R(6) * c.w + R(2) * c.z);
+  fph = d0 + t * (R(2) * c.z + t * d2);
+  return c.x + t * (c.y + t * (c.z + t * c.w));
 }
 
 template <typename R>
@@ -723,14 +687,26 @@ __device__ __forceinline__ void chunk_range(int p0, int p1, int c, int nch, int 
 /* ------------------------------------------------------------------------ */
 #define ITILE 128
 
+/* a staged partner: position and 1/(R h) in one vector record, the
+   descreening weight and radius type in another */
+template <typename R>
+struct alignas(4 * sizeof(R)) Part4 {
+  R x, y, z, rh;
+};
+template <typename R>
+struct alignas(2 * sizeof(R)) PartW {
+  R w;
+  int t;
+};
+
 template <typename R>
 __global__ void __launch_bounds__(ITILE) k_descreen_t(View v, const int4 *__restrict__ items, int nitems,
                                                       int nch) {
-  AGB_SHARED R sx[ITILE], sy[ITILE], sz[ITILE], srh[ITILE], sw[ITILE];
-  AGB_SHARED int st[ITILE];
+  AGB_SHARED Part4<R> sp4[ITILE];
+  AGB_SHARED PartW<R> spw[ITILE];
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
   const R *RH = pa<R>(v, PA_RH), *W = pa<R>(v, PA_W);
-  const typename Rec4<R>::T *tab = tables4<R>(v);
+  const typename Tab<R>::T *tab = Tab<R>::val(v);
   const int nt = v.ntypes;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     int4 w = items[it];
@@ -745,22 +721,27 @@ __global__ void __launch_bounds__(ITILE) k_descreen_t(View v, const int4 *__rest
       int n = min(ITILE, c1 - j0);
       AGB_SYNC();
       AGB_COOP_FOR(t, n) {
-        sx[t] = X[j0 + t];
-        sy[t] = Y[j0 + t];
-        sz[t] = Z[j0 + t];
-        srh[t] = RH[j0 + t];
-        sw[t] = W[j0 + t];
-        st[t] = v.rtype[j0 + t];
+        Part4<R> a;
+        a.x = X[j0 + t];
+        a.y = Y[j0 + t];
+        a.z = Z[j0 + t];
+        a.rh = RH[j0 + t];
+        sp4[t] = a;
+        PartW<R> b;
+        b.w = W[j0 + t];
+        b.t = v.rtype[j0 + t];
+        spw[t] = b;
       }
       AGB_SYNC();
       if (act) {
         R part = R(0);
         for (int t = 0; t < n; t++) {
-          R dx = sx[t] - xg, dy = sy[t] - yg, dz = sz[t] - zg;
-          R xh = m_sqrt(dx * dx + dy * dy + dz * dz) * srh[t];
+          Part4<R> a = sp4[t];
+          R dx = a.x - xg, dy = a.y - yg, dz = a.z - zg;
+          R xh = m_sqrt(dx * dx + dy * dy + dz * dz) * a.rh;
           if (xh < R(AGB_NA - 1) && j0 + t != g) {
-            R fp;
-            part += sw[t] * spline<R>(tab, row + st[t], xh, fp, false, false);
+            PartW<R> b = spw[t];
+            part += b.w * spline<R>(tab, row + b.t, xh);
           }
         }
         acc += (double)part;
@@ -900,9 +881,9 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
   const R *RH = pa<R>(v, PA_RH), *RI = pa<R>(v, PA_RINV), *SP = pa<R>(v, PA_SP);
   const R *Q2 = pa<R>(v, PA_Q2AB), *AB = pa<R>(v, PA_ABRW);
-  const typename Rec4<R>::T *tab = tables4<R>(v);
+  const typename Tab<R>::T *tv = Tab<R>::val(v);
+  const R kref = v.compat ? R(1) : R(0), hinv = R((AGB_NA - 1) / C_AMAX);
   const int nt = v.ntypes;
-  const bool rs = v.compat != 0;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     int4 w = items[it];
     int g = w.y + threadIdx.x;
@@ -947,8 +928,8 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
             R xh = d * rhg;
             if (xh < R(AGB_NA - 1)) {
               R fp;
-              R f = spline<R>(tab, st[t] * nt + tg, xh, fp, true, rs);
-              R q = f * rig, dq = fp * rig * rig;
+              R f = spline_d<R>(tv, st[t] * nt + tg, xh, kref, fp);
+              R q = f * rig, dq = fp * hinv * rig * rig;
               pu += sq2[t] * q;
               pv += sab[t] * q;
               ht += sq2[t] * dq * spg;
@@ -959,8 +940,8 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
             R xh = d * srh[t];
             if (xh < R(AGB_NA - 1)) {
               R fp;
-              spline<R>(tab, tg * nt + st[t], xh, fp, true, rs);
-              R dq = fp * sri[t] * sri[t] * ssp[t];
+              spline_d<R>(tv, tg * nt + st[t], xh, kref, fp);
+              R dq = fp * hinv * sri[t] * sri[t] * ssp[t];
               ht += q2g * dq;
               ut += abg * dq;
             }
@@ -1107,9 +1088,9 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
   const R *RH = pa<R>(v, PA_RH), *RI = pa<R>(v, PA_RINV), *SP = pa<R>(v, PA_SP);
   const R *Q2 = pa<R>(v, PA_Q2AB), *AB = pa<R>(v, PA_ABRW);
-  const typename Rec4<R>::T *tab = tables4<R>(v);
+  const typename Tab<R>::T *tv = Tab<R>::val(v);
+  const R kref = v.compat ? R(1) : R(0), hinv = R((AGB_NA - 1) / C_AMAX);
   const int nt = v.ntypes;
-  const bool rs = v.compat != 0;
   for (int it = blockIdx.x * 4 + (threadIdx.x >> 5); it < nitems; it += gridDim.x * 4) {
     int4 w = items[it];
     int a0 = v.inst_begin[w.x], hh = a0 + v.inst_nheavy[w.x], a1 = v.inst_begin[w.x + 1];
@@ -1155,8 +1136,8 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
           R xh = d * rhi;
           if (xh < R(AGB_NA - 1)) {
             R fp;
-            R f = spline<R>(tab, tj * nt + ti, xh, fp, true, rs);
-            R q = f * rii, dq = fp * rii * rii;
+            R f = spline_d<R>(tv, tj * nt + ti, xh, kref, fp);
+            R q = f * rii, dq = fp * hinv * rii * rii;
             pU += q2j * q;
             pV += abj * q;
             ht += q2j * dq * spi;
@@ -1167,8 +1148,8 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
           R xh = d * rhj;
           if (xh < R(AGB_NA - 1)) {
             R fp;
-            R f = spline<R>(tab, ti * nt + tj, xh, fp, true, rs);
-            R q = f * rij, dq = fp * rij * rij;
+            R f = spline_d<R>(tv, ti * nt + tj, xh, kref, fp);
+            R q = f * rij, dq = fp * hinv * rij * rij;
             jU += q2i * q;
             jV += abi * q;
             ht += q2i * dq * spj;
@@ -2026,9 +2007,6 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     for (int w = d->ws_begin[I]; w < d->ws_begin[I + 1]; w++) ws_inst[w] = I;
   double *vols = (double *)malloc(sizeof(double) * N);
   for (int g = 0; g < N; g++) vols[g] = 4.0 * C_PI / 3.0 * d->r[g] * d->r[g] * d->r[g];
-  size_t ntab = (size_t)d->ntypes * d->ntypes * AGB_NA * 2;
-  float *tabf = (float *)malloc(sizeof(float) * ntab);
-  for (size_t k = 0; k < ntab; k++) tabf[k] = (float)d->tab[k];
 
 #define UP(field, src, n, T)                     \
   do {                                           \
@@ -2053,28 +2031,31 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   UP(salpha, d->salpha, N, double);
   UP(vols, vols, N, double);
   UP(rtype, d->rtype, N, int);
-  UP(tab_d, d->tab, ntab, double);
-  UP(tab_f, tabf, ntab, float);
   {
-    /* one record per interval: y_k, y2_k, y_k+1, y2_k+1 (the last node's
-       record is never read: a lookup stops below node AGB_NA-1) */
-    size_t nslot = (size_t)d->ntypes * d->ntypes;
-    double *t4 = (double *)calloc(nslot * AGB_NA * 4, sizeof(double));
-    float *t4f = (float *)calloc(nslot * AGB_NA * 4, sizeof(float));
-    for (size_t sl = 0; sl < nslot; sl++)
-      for (int k = 0; k + 1 < AGB_NA; k++) {
-        const double *a = d->tab + (sl * AGB_NA + k) * 2;
-        double *o = t4 + (sl * AGB_NA + k) * 4;
-        o[0] = a[0];
-        o[1] = a[1];
-        o[2] = a[2];
-        o[3] = a[3];
-        for (int c = 0; c < 4; c++) t4f[(sl * AGB_NA + k) * 4 + c] = (float)o[c];
+    /* per interval k, from the node values y and second derivatives y2 of
+       the spline in a (step h), with t = a/h - k:
+         f(t) = c0 + c1 t + c2 t^2 + c3 t^3,
+         c0 = y_k,  c1 = y_k+1 - y_k - h^2 (2 y2_k + y2_k+1) / 6,
+         c2 = h^2 y2_k / 2,  c3 = h^2 (y2_k+1 - y2_k) / 6.
+       The last node's record is never read: a lookup stops below node
+       AGB_NA-1. */
+    size_t nrec = (size_t)d->ntypes * d->ntypes * AGB_NA;
+    double *tv = (double *)calloc(nrec * 4, sizeof(double));
+    float *fv = (float *)calloc(nrec * 4, sizeof(float));
+    const double h = C_AMAX / (AGB_NA - 1), hh6 = h * h / 6.0;
+    for (size_t q = 0; q < nrec; q++) {
+      if ((int)(q % AGB_NA) == AGB_NA - 1) continue;
+      const double *a = d->tab + q * 2; /* y_k, y2_k, y_k+1, y2_k+1 */
+      double c[4] = {a[0], a[2] - a[0] - hh6 * (2.0 * a[1] + a[3]), 0.5 * h * h * a[1], hh6 * (a[3] - a[1])};
+      for (int k = 0; k < 4; k++) {
+        tv[4 * q + k] = c[k];
+        fv[4 * q + k] = (float)c[k];
       }
-    UP(tab4_d, t4, nslot * AGB_NA * 4, double);
-    UP(tab4_f, t4f, nslot * AGB_NA * 4, float);
-    free(t4);
-    free(t4f);
+    }
+    UP(tabv_d, (const double4 *)tv, nrec, double4);
+    UP(tabv_f, (const float4 *)fv, nrec, float4);
+    free(tv);
+    free(fv);
   }
   UP(ws_begin, d->ws_begin, NI + 1, int);
   if (NW > 0) {
@@ -2090,7 +2071,6 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   free(bucket_mask);
   free(ws_inst);
   free(vols);
-  free(tabf);
 
   /* per-evaluation buffers */
   DALLOC(v.x_ext, N, double);
