@@ -36,6 +36,7 @@
 #include "agbnp3_dev.h"
 
 #include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -983,13 +984,14 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
 }
 
 /* ------------------------------------------------------------------------ */
-/* symmetric pair passes: each warp owns a 32-atom i tile and walks a run of */
-/* 32-atom j tiles (j >= i tile) of the same instance.  Lane l keeps atom i; */
-/* the j atoms' operands and their partial sums rotate through the warp with */
-/* __shfl_sync, so every unordered pair is evaluated exactly once and each j */
-/* atom's sums return to their lane after 32 rotations.  On a diagonal tile  */
-/* the rotations 1..16 cover each pair once (rotation 16 only on lanes < 16).*/
-/* Partial sums are float per tile pair, then double.                        */
+/* symmetric pair passes: each warp owns a 64-atom i block (lane l keeps     */
+/* atoms I+l and I+32+l) and walks a run of 32-atom j tiles of the same      */
+/* instance starting at the block.  The j atoms' operands and their partial  */
+/* sums rotate through the warp with __shfl_sync: in step r lane l holds j   */
+/* atom J+((l+r) mod 32), evaluates its pairs with both i atoms when i < j,  */
+/* and after 32 steps each j atom's sums are back in its lane.  Every        */
+/* unordered pair is evaluated once, two per lane and step.  Partial sums    */
+/* are float per j tile, then double.                                        */
 /* ------------------------------------------------------------------------ */
 #define FULLMASK 0xffffffffu
 
@@ -1007,53 +1009,60 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
   const R *Q = pa<R>(v, PA_Q), *Bv = pa<R>(v, PA_B), *BI = pa<R>(v, PA_BINV);
   size_t N = v.natoms;
   for (int it = blockIdx.x * 4 + (threadIdx.x >> 5); it < nitems; it += gridDim.x * 4) {
-    int4 w = items[it]; /* instance, first atom of the i tile, first atom of the j run, j tiles */
-    int a1 = v.inst_begin[w.x + 1];
-    int i = w.y + lane;
-    bool vi = i < a1;
-    R xi = vi ? X[i] : R(1e6), yi = vi ? Y[i] : R(0), zi = vi ? Z[i] : R(0);
-    R qi = vi ? Q[i] : R(0), bi = vi ? Bv[i] : R(1), ci = vi ? GbExp<R>::scale() * BI[i] : R(0);
-    double se = 0, sgx = 0, sgy = 0, sgz = 0, sat = 0;
+    int4 w = items[it]; /* instance, first atom of the i block, first atom of the j run, j tiles */
+    const int a1 = v.inst_begin[w.x + 1];
+    int ia[2];
+    R xi[2], yi[2], zi[2], qi[2], bi[2], ci[2];
+    double se[2], sgx[2], sgy[2], sgz[2], sat[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      ia[u] = w.y + 32 * u + lane;
+      bool ok = ia[u] < a1;
+      xi[u] = ok ? X[ia[u]] : R(0);
+      yi[u] = ok ? Y[ia[u]] : R(0);
+      zi[u] = ok ? Z[ia[u]] : R(0);
+      qi[u] = ok ? Q[ia[u]] : R(0);
+      bi[u] = ok ? Bv[ia[u]] : R(1);
+      ci[u] = ok ? GbExp<R>::scale() * BI[ia[u]] : R(0);
+      if (!ok) ia[u] = INT_MAX; /* no valid partner: i < j never holds */
+      se[u] = sgx[u] = sgy[u] = sgz[u] = sat[u] = 0.0;
+    }
     for (int k = 0; k < w.w; k++) {
-      int j0 = w.z + 32 * k;
+      const int j0 = w.z + 32 * k;
       int j = j0 + lane;
       bool vj = j < a1;
-      R xj = vj ? X[j] : R(-1e6), yj = vj ? Y[j] : R(0), zj = vj ? Z[j] : R(0);
+      R xj = vj ? X[j] : R(0), yj = vj ? Y[j] : R(0), zj = vj ? Z[j] : R(0);
       R qj = vj ? Q[j] : R(0), bj = vj ? Bv[j] : R(1), bij = vj ? BI[j] : R(0);
       R jgx = 0, jgy = 0, jgz = 0, jat = 0;
-      R pe = 0, pgx = 0, pgy = 0, pgz = 0, pat = 0;
-      const bool diag = j0 == w.y;
-      const int nrot = diag ? 16 : 32;
-      for (int r = diag ? 1 : 0; r <= nrot; r++) {
+      R pe[2] = {0, 0}, pgx[2] = {0, 0}, pgy[2] = {0, 0}, pgz[2] = {0, 0}, pat[2] = {0, 0};
+      for (int r = 0; r < 32; r++) {
         if (r > 0) {
           xj = rot1(xj); yj = rot1(yj); zj = rot1(zj);
           qj = rot1(qj); bj = rot1(bj); bij = rot1(bij);
-          jgx = rot1(jgx); jgy = rot1(jgy); jgz = rot1(jgz); jat = rot1(jat);
         }
-        if (r == 32 || (diag && r == 16 && lane >= 16)) continue;
-        R dx = xj - xi, dy = yj - yi, dz = zj - zi;
-        R d2 = dx * dx + dy * dy + dz * dz;
-        if (!(d2 > R(0)) || d2 > R(1e10)) continue; /* same / coincident / padding atoms */
-        R bb = bi * bj;
-        R et = GbExp<R>::ex(ci * bij * d2);
-        R f = m_rsqrt(d2 + bb * et);
-        R qq = qi * qj;
-        R qf3 = qq * f * f * f;
-        pe += qq * f;
-        R mw = (R(1) - R(0.25) * et) * qf3;
-        R gx = mw * dx, gy = mw * dy, gz = mw * dz;
-        pgx += gx; pgy += gy; pgz += gz;
-        jgx -= gx; jgy -= gy; jgz -= gz;
-        R at = (bb + R(0.25) * d2) * et * qf3;
-        pat += at;
-        jat += at;
-      }
-      if (diag) { /* 16 rotations: the j sums sit 16 lanes away */
-        int src = (lane + 16) & 31;
-        jgx = __shfl_sync(FULLMASK, jgx, src);
-        jgy = __shfl_sync(FULLMASK, jgy, src);
-        jgz = __shfl_sync(FULLMASK, jgz, src);
-        jat = __shfl_sync(FULLMASK, jat, src);
+        const int jr = j0 + ((lane + r) & 31);
+        const bool jok = jr < a1;
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          R dx = xj - xi[u], dy = yj - yi[u], dz = zj - zi[u];
+          R d2 = dx * dx + dy * dy + dz * dz;
+          if (jok && ia[u] < jr && d2 > R(0)) { /* coincident atoms are skipped */
+            R bb = bi[u] * bj;
+            R et = GbExp<R>::ex(ci[u] * bij * d2);
+            R f = m_rsqrt(d2 + bb * et);
+            R qq = qi[u] * qj;
+            R qf3 = qq * f * f * f;
+            pe[u] += qq * f;
+            R mw = (R(1) - R(0.25) * et) * qf3;
+            R gx = mw * dx, gy = mw * dy, gz = mw * dz;
+            pgx[u] += gx; pgy[u] += gy; pgz[u] += gz;
+            jgx -= gx; jgy -= gy; jgz -= gz;
+            R at = (bb + R(0.25) * d2) * et * qf3;
+            pat[u] += at;
+            jat += at;
+          }
+        }
+        jgx = rot1(jgx); jgy = rot1(jgy); jgz = rot1(jgz); jat = rot1(jat);
       }
       if (vj) {
         double w2 = 2.0 * v.inst_df[w.x];
@@ -1062,26 +1071,31 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
         atomicAdd(&v.g_gb[3 * j + 2], w2 * (double)jgz);
         atomicAdd(&v.dera[j], (double)jat);
       }
-      se += (double)pe;
-      sgx += (double)pgx;
-      sgy += (double)pgy;
-      sgz += (double)pgz;
-      sat += (double)pat;
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        se[u] += (double)pe[u];
+        sgx[u] += (double)pgx[u];
+        sgy[u] += (double)pgy[u];
+        sgz[u] += (double)pgz[u];
+        sat[u] += (double)pat[u];
+      }
     }
-    if (vi) {
-      double w2 = 2.0 * v.inst_df[w.x];
-      atomicAdd(&v.eatom[N + i], C_TOKCAL * w2 * se);
-      atomicAdd(&v.g_gb[3 * i], w2 * sgx);
-      atomicAdd(&v.g_gb[3 * i + 1], w2 * sgy);
-      atomicAdd(&v.g_gb[3 * i + 2], w2 * sgz);
-      atomicAdd(&v.dera[i], sat);
+    const double w2 = 2.0 * v.inst_df[w.x];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      int i = ia[u];
+      if (i >= a1) continue;
+      atomicAdd(&v.eatom[N + i], C_TOKCAL * w2 * se[u]);
+      atomicAdd(&v.g_gb[3 * i], w2 * sgx[u]);
+      atomicAdd(&v.g_gb[3 * i + 1], w2 * sgy[u]);
+      atomicAdd(&v.g_gb[3 * i + 2], w2 * sgz[u]);
+      atomicAdd(&v.dera[i], sat[u]);
     }
   }
 }
 
-/* gbders: both descreening directions of every unordered pair, pair forces,
-   U and V (agbnp3_cpu_simd_kernels.c:681-904); flags: bit 0 valid, bit 1
-   heavy */
+/* gbders: both descreening directions of every unordered pair with a heavy
+   atom, pair forces, U and V (agbnp3_cpu_simd_kernels.c:681-904) */
 template <typename R>
 __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restrict__ items, int nitems) {
   const int lane = threadIdx.x & 31;
@@ -1093,88 +1107,91 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
   const int nt = v.ntypes;
   for (int it = blockIdx.x * 4 + (threadIdx.x >> 5); it < nitems; it += gridDim.x * 4) {
     int4 w = items[it];
-    int a0 = v.inst_begin[w.x], hh = a0 + v.inst_nheavy[w.x], a1 = v.inst_begin[w.x + 1];
-    int i = w.y + lane;
-    bool vi = i < a1, hi = i < hh;
-    R xi = vi ? X[i] : R(0), yi = vi ? Y[i] : R(0), zi = vi ? Z[i] : R(0);
-    R rhi = vi ? RH[i] : R(0), rii = vi ? RI[i] : R(0), spi = vi ? SP[i] : R(0);
-    R q2i = vi ? Q2[i] : R(0), abi = vi ? AB[i] : R(0);
-    int ti = vi ? v.rtype[i] : 0;
-    double sU = 0, sV = 0, sfx = 0, sfy = 0, sfz = 0, svx = 0, svy = 0, svz = 0;
+    const int a0 = v.inst_begin[w.x], hh = a0 + v.inst_nheavy[w.x], a1 = v.inst_begin[w.x + 1];
+    int ia[2], ti[2];
+    bool hi[2];
+    R xi[2], yi[2], zi[2], rhi[2], rii[2], spi[2], q2i[2], abi[2];
+    double sU[2], sV[2], sfx[2], sfy[2], sfz[2], svx[2], svy[2], svz[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      int i = w.y + 32 * u + lane;
+      bool ok = i < a1;
+      hi[u] = i < hh;
+      xi[u] = ok ? X[i] : R(0);
+      yi[u] = ok ? Y[i] : R(0);
+      zi[u] = ok ? Z[i] : R(0);
+      rhi[u] = ok ? RH[i] : R(0);
+      rii[u] = ok ? RI[i] : R(0);
+      spi[u] = ok ? SP[i] : R(0);
+      q2i[u] = ok ? Q2[i] : R(0);
+      abi[u] = ok ? AB[i] : R(0);
+      ti[u] = ok ? v.rtype[i] : 0;
+      ia[u] = ok ? i : INT_MAX; /* no valid partner: i < j never holds */
+      sU[u] = sV[u] = sfx[u] = sfy[u] = sfz[u] = svx[u] = svy[u] = svz[u] = 0.0;
+    }
     for (int k = 0; k < w.w; k++) {
-      int j0 = w.z + 32 * k;
+      const int j0 = w.z + 32 * k;
       int j = j0 + lane;
       bool vj = j < a1;
       R xj = vj ? X[j] : R(0), yj = vj ? Y[j] : R(0), zj = vj ? Z[j] : R(0);
       R rhj = vj ? RH[j] : R(0), rij = vj ? RI[j] : R(0), spj = vj ? SP[j] : R(0);
       R q2j = vj ? Q2[j] : R(0), abj = vj ? AB[j] : R(0);
-      int fj = vj ? (v.rtype[j] << 2) | 1 | (j < hh ? 2 : 0) : 0;
+      int tj = vj ? v.rtype[j] : 0;
       R jU = 0, jV = 0, jfx = 0, jfy = 0, jfz = 0, jvx = 0, jvy = 0, jvz = 0;
-      R pU = 0, pV = 0, pfx = 0, pfy = 0, pfz = 0, pvx = 0, pvy = 0, pvz = 0;
-      const bool diag = j0 == w.y;
-      const int nrot = diag ? 16 : 32;
-      for (int r = diag ? 1 : 0; r <= nrot; r++) {
+      R pU[2] = {0, 0}, pV[2] = {0, 0}, pfx[2] = {0, 0}, pfy[2] = {0, 0}, pfz[2] = {0, 0};
+      R pvx[2] = {0, 0}, pvy[2] = {0, 0}, pvz[2] = {0, 0};
+      for (int r = 0; r < 32; r++) {
         if (r > 0) {
           xj = rot1(xj); yj = rot1(yj); zj = rot1(zj);
           rhj = rot1(rhj); rij = rot1(rij); spj = rot1(spj);
-          q2j = rot1(q2j); abj = rot1(abj); fj = rot1(fj);
-          jU = rot1(jU); jV = rot1(jV);
-          jfx = rot1(jfx); jfy = rot1(jfy); jfz = rot1(jfz);
-          jvx = rot1(jvx); jvy = rot1(jvy); jvz = rot1(jvz);
+          q2j = rot1(q2j); abj = rot1(abj); tj = rot1(tj);
         }
-        if (r == 32 || (diag && r == 16 && lane >= 16)) continue;
-        bool hj = (fj & 2) != 0;
-        if (!vi || !(fj & 1) || !(hi || hj)) continue;
-        R dx = xj - xi, dy = yj - yi, dz = zj - zi;
-        R d2 = dx * dx + dy * dy + dz * dz;
-        if (!(d2 > R(0))) continue;
-        R id = m_rsqrt(d2);
-        R d = d2 * id;
-        int tj = fj >> 2;
-        R ht = R(0), ut = R(0);
-        if (hi) { /* j descreened by i: table (type j, type i), radius of i */
-          R xh = d * rhi;
-          if (xh < R(AGB_NA - 1)) {
-            R fp;
-            R f = spline_d<R>(tv, tj * nt + ti, xh, kref, fp);
-            R q = f * rii, dq = fp * hinv * rii * rii;
-            pU += q2j * q;
-            pV += abj * q;
-            ht += q2j * dq * spi;
-            ut += abj * dq * spi;
+        const int jr = j0 + ((lane + r) & 31);
+        const bool jok = jr < a1, hj = jr < hh;
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          R dx = xj - xi[u], dy = yj - yi[u], dz = zj - zi[u];
+          R d2 = dx * dx + dy * dy + dz * dz;
+          if (!(jok && ia[u] < jr && (hi[u] || hj) && d2 > R(0))) continue;
+          R id = m_rsqrt(d2);
+          R d = d2 * id;
+          R ht = R(0), ut = R(0);
+          if (hi[u]) { /* j descreened by i: table (type j, type i), radius of i */
+            R xh = d * rhi[u];
+            if (xh < R(AGB_NA - 1)) {
+              R fp;
+              R f = spline_d<R>(tv, tj * nt + ti[u], xh, kref, fp);
+              R q = f * rii[u], dq = fp * hinv * rii[u] * rii[u];
+              pU[u] += q2j * q;
+              pV[u] += abj * q;
+              ht += q2j * dq * spi[u];
+              ut += abj * dq * spi[u];
+            }
           }
-        }
-        if (hj) { /* i descreened by j: table (type i, type j), radius of j */
-          R xh = d * rhj;
-          if (xh < R(AGB_NA - 1)) {
-            R fp;
-            R f = spline_d<R>(tv, ti * nt + tj, xh, kref, fp);
-            R q = f * rij, dq = fp * hinv * rij * rij;
-            jU += q2i * q;
-            jV += abi * q;
-            ht += q2i * dq * spj;
-            ut += abi * dq * spj;
+          if (hj) { /* i descreened by j: table (type i, type j), radius of j */
+            R xh = d * rhj;
+            if (xh < R(AGB_NA - 1)) {
+              R fp;
+              R f = spline_d<R>(tv, ti[u] * nt + tj, xh, kref, fp);
+              R q = f * rij, dq = fp * hinv * rij * rij;
+              jU += q2i[u] * q;
+              jV += abi[u] * q;
+              ht += q2i[u] * dq * spj;
+              ut += abi[u] * dq * spj;
+            }
           }
+          ht *= id;
+          ut *= id;
+          R fx = ht * dx, fy = ht * dy, fz = ht * dz;
+          R ux = ut * dx, uy = ut * dy, uz = ut * dz;
+          pfx[u] += fx; pfy[u] += fy; pfz[u] += fz;
+          pvx[u] += ux; pvy[u] += uy; pvz[u] += uz;
+          jfx -= fx; jfy -= fy; jfz -= fz;
+          jvx -= ux; jvy -= uy; jvz -= uz;
         }
-        ht *= id;
-        ut *= id;
-        R fx = ht * dx, fy = ht * dy, fz = ht * dz;
-        R ux = ut * dx, uy = ut * dy, uz = ut * dz;
-        pfx += fx; pfy += fy; pfz += fz;
-        pvx += ux; pvy += uy; pvz += uz;
-        jfx -= fx; jfy -= fy; jfz -= fz;
-        jvx -= ux; jvy -= uy; jvz -= uz;
-      }
-      if (diag) {
-        int src = (lane + 16) & 31;
-        jU = __shfl_sync(FULLMASK, jU, src);
-        jV = __shfl_sync(FULLMASK, jV, src);
-        jfx = __shfl_sync(FULLMASK, jfx, src);
-        jfy = __shfl_sync(FULLMASK, jfy, src);
-        jfz = __shfl_sync(FULLMASK, jfz, src);
-        jvx = __shfl_sync(FULLMASK, jvx, src);
-        jvy = __shfl_sync(FULLMASK, jvy, src);
-        jvz = __shfl_sync(FULLMASK, jvz, src);
+        jU = rot1(jU); jV = rot1(jV);
+        jfx = rot1(jfx); jfy = rot1(jfy); jfz = rot1(jfz);
+        jvx = rot1(jvx); jvy = rot1(jvy); jvz = rot1(jvz);
       }
       const double f4p = 1.0 / (4.0 * C_PI), kg = f4p * v.inst_df[w.x];
       if (vj) {
@@ -1189,26 +1206,32 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
           atomicAdd(&v.derv[j], (double)jV);
         }
       }
-      sU += (double)pU;
-      sV += (double)pV;
-      sfx += (double)pfx;
-      sfy += (double)pfy;
-      sfz += (double)pfz;
-      svx += (double)pvx;
-      svy += (double)pvy;
-      svz += (double)pvz;
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        sU[u] += (double)pU[u];
+        sV[u] += (double)pV[u];
+        sfx[u] += (double)pfx[u];
+        sfy[u] += (double)pfy[u];
+        sfz[u] += (double)pfz[u];
+        svx[u] += (double)pvx[u];
+        svy[u] += (double)pvy[u];
+        svz[u] += (double)pvz[u];
+      }
     }
-    if (vi) {
-      const double f4p = 1.0 / (4.0 * C_PI), kg = f4p * v.inst_df[w.x];
-      atomicAdd(&v.g_gb[3 * i], kg * sfx);
-      atomicAdd(&v.g_gb[3 * i + 1], kg * sfy);
-      atomicAdd(&v.g_gb[3 * i + 2], kg * sfz);
-      atomicAdd(&v.g_vw[3 * i], f4p * svx);
-      atomicAdd(&v.g_vw[3 * i + 1], f4p * svy);
-      atomicAdd(&v.g_vw[3 * i + 2], f4p * svz);
-      if (hi) {
-        atomicAdd(&v.deru[i], sU);
-        atomicAdd(&v.derv[i], sV);
+    const double f4p = 1.0 / (4.0 * C_PI), kg = f4p * v.inst_df[w.x];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      int i = ia[u];
+      if (i >= a1) continue;
+      atomicAdd(&v.g_gb[3 * i], kg * sfx[u]);
+      atomicAdd(&v.g_gb[3 * i + 1], kg * sfy[u]);
+      atomicAdd(&v.g_gb[3 * i + 2], kg * sfz[u]);
+      atomicAdd(&v.g_vw[3 * i], f4p * svx[u]);
+      atomicAdd(&v.g_vw[3 * i + 1], f4p * svy[u]);
+      atomicAdd(&v.g_vw[3 * i + 2], f4p * svz[u]);
+      if (hi[u]) {
+        atomicAdd(&v.deru[i], sU[u]);
+        atomicAdd(&v.derv[i], sV[u]);
       }
     }
   }
@@ -1913,25 +1936,27 @@ static int build_items(agb_dev *s, int nch, int jb) {
         it[q].w = c;
         q++;
       }
+  /* symmetric items: 64-atom i blocks, runs of up to jb 32-atom j tiles
+     from the block's first tile to the end of the instance */
   int cap = 0;
   for (int I = 0; I < NI; I++) {
     int T = (ib[I + 1] - ib[I] + 31) / 32;
-    cap += T * ((T + jb - 1) / jb);
+    for (int tb = 0; tb < T; tb += 2) cap += (T - tb + jb - 1) / jb;
   }
   int4 *ia = (int4 *)malloc(sizeof(int4) * (cap + 1)), *ig = (int4 *)malloc(sizeof(int4) * (cap + 1));
   int na = 0, ng = 0;
   for (int I = 0; I < NI; I++) {
     int a0 = ib[I], n = ib[I + 1] - a0, T = (n + 31) / 32;
     int hh = a0 + inh[I];
-    for (int ti = 0; ti < T; ti++)
-      for (int tj = ti; tj < T; tj += jb) {
+    for (int tb = 0; tb < T; tb += 2)
+      for (int tj = tb; tj < T; tj += jb) {
         int4 w;
         w.x = I;
-        w.y = a0 + 32 * ti;
+        w.y = a0 + 32 * tb;
         w.z = a0 + 32 * tj;
         w.w = (T - tj) < jb ? (T - tj) : jb;
         ia[na++] = w;
-        if (w.y < hh) ig[ng++] = w;
+        if (w.y < hh) ig[ng++] = w; /* blocks of hydrogens only have no gbders pairs */
       }
   }
   if (s->items) cudaFree(s->items);
