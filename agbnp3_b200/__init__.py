@@ -91,6 +91,7 @@ def lib():
         L.agbnp3_batch_stage_times.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         L.agbnp3_autotune.argtypes = [ctypes.c_int, _ip, ctypes.c_int]
         L.agbnp3_batch_autotune.argtypes = [ctypes.c_int, _ip, ctypes.c_int]
+        L.agbnp3_measure_peaks.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -110,6 +111,16 @@ def _p(a, t=_dp):
 
 def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def measure_peaks(device: int = 0) -> dict:
+    """FP32 / FP64 flop/s (FMA = 2 flops) and ex2 op/s of the GPU, measured
+    by the library's own throughput kernels (agbnp3_measure_peaks)."""
+    out = np.zeros(4)
+    if lib().agbnp3_measure_peaks(device, _p(out), 4) != 4:
+        raise AGBNPError("agbnp3_measure_peaks failed")
+    return {"fp32_tflops": out[0] / 1e12, "fp64_tflops": out[1] / 1e12, "ex2_tops": out[2] / 1e12,
+            "nominal_sm_mhz": out[3]}
 
 
 def initialize():

@@ -35,12 +35,12 @@ UNIT = "evals/s"
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--natoms", type=int, default=25000)
     p.add_argument("--seed", type=int, default=1)
-    p.add_argument("--fp64-steps", type=int, default=5)
+    p.add_argument("--fp64-steps", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--config", default="globule25k", choices=["globule25k", "batch512"],
                    help="globule25k: one 25,000-atom globule (headline); batch512: 512 instances of "
@@ -156,6 +156,44 @@ def reference_arm(args):
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
                          "sample": f"{args.steps} full evaluations of the {args.natoms}-atom globule"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# Operations per pair of each pair stage, counted from the stage's formulas
+# (an FMA counts as two flops; add, multiply and compare-free selects one):
+#   descreening (invb), atom i by heavy atom j: distance 8, sqrt (SFU),
+#     a/h 1, interval offset 1, cubic 6, weighted sum 2            = 18 + 1 SFU
+#   GB pair energy (agb), unordered pair: distance 8, BiBj 1, exponent 2,
+#     exp2 (SFU), d^2 + BiBj e 2, rsqrt (SFU), qiqj 1, q f^3 3, energy 2,
+#     force weight 3, force 3 + 6 sums, A_i term 4 + 2 sums       = 37 + 2 SFU
+#   Born-radius chain rule (gbders), per direction with a heavy descreener:
+#     a/h 1, offset 1, cubic 6, derivative 6, Q 1, dQ 3, U, V 4, force
+#     weights 6 = 28; per pair: distance 8, rsqrt (SFU), d 1, scaling 2,
+#     force components 6, 12 sums = 29 + 1 SFU; heavy-heavy pairs have two
+#     directions, heavy-hydrogen pairs one
+PAIR_OPS = {"invb": (18, 1), "agb": (37, 2), "gbders_hh": (29 + 2 * 28, 1), "gbders_hx": (29 + 28, 1)}
+
+
+def pair_roofline(natoms, nheavy, stage_ms, peaks):
+    nx = natoms - nheavy
+    work = {  # (flops, SFU ops) per launch
+        "invb": [(natoms * nheavy - nheavy) * w for w in PAIR_OPS["invb"]],
+        "agb": [natoms * (natoms - 1) // 2 * w for w in PAIR_OPS["agb"]],
+        "gbders": [nheavy * (nheavy - 1) // 2 * a + nheavy * nx * b
+                   for a, b in zip(PAIR_OPS["gbders_hh"], PAIR_OPS["gbders_hx"])],
+    }
+    stages = {}
+    for k, (fl, sf) in work.items():
+        t = stage_ms[k] * 1e-3
+        stages[k] = {"gflop_per_launch": fl / 1e9, "ms": stage_ms[k], "tflops": fl / t / 1e12,
+                     "fp32_frac": fl / t / 1e12 / peaks["fp32_tflops"],
+                     "sfu_frac": sf / t / 1e12 / peaks["ex2_tops"]}
+    dom = max(stages, key=lambda k: stages[k]["ms"])
+    d = stages[dom]
+    return {"kernel": {"gbders": "k_gbders_sym", "agb": "k_agb_sym", "invb": "k_descreen_t"}[dom],
+            "stage": dom, "bound": "fp32", "achieved": d["tflops"], "peak": peaks["fp32_tflops"],
+            "unit": "TFLOP/s", "frac": d["fp32_frac"], "traffic": None,
+            "peak_source": "measured in this run: FP32 FMA chains on every SM (agbnp3_measure_peaks)",
+            "sfu_frac": d["sfu_frac"], "peaks": peaks, "stages": stages}
 
 
 def batch_systems(A, ninst, seed, rank=0):
@@ -359,18 +397,11 @@ def main():
     e2e_tot = max_over_ranks(sum(e2e_t), world, f"cuda:{local}")
     e2e_value = throughput(args.steps, e2e_tot, world)
 
-    # dominant stage and its arithmetic rate (pair counts x
-    # frozen per-pair operation weights)
-    nh = s.nheavy
-    pairs = {"agb": natoms * (natoms - 1), "invb": natoms * nh, "gbders": 2 * nh * (natoms - 1)}
-    flops_per_pair = {"agb": 30, "invb": 32, "gbders": 40}
-    dom = max(stage_ms, key=stage_ms.get)
-    roof = None
-    if dom in pairs:
-        achieved = pairs[dom] * flops_per_pair[dom] / (stage_ms[dom] * 1e-3) / 1e12
-        roof = {"kernel": dom, "bound": "fp32", "achieved": achieved, "unit": "TFLOP/s",
-                "peak": None, "frac": None, "traffic": None,
-                "note": "FP32 issue bound; peak from the FP32 FMA microbenchmark when available"}
+    # roofline of the pair stages: algorithmic FP32 work per launch (pair
+    # counts x frozen per-pair operation counts) over the stage's device
+    # time, against FP32 / special-function peaks measured in this run
+    peaks = A.measure_peaks(local)
+    roof = pair_roofline(natoms, s.nheavy, stage_ms, peaks)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and os.path.exists(os.path.join(ROOT, "oracle", "_ref",

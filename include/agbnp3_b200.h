@@ -104,6 +104,13 @@ int agbnp3_gb_energy_static(int natoms, const double *x, const double *y, const 
                             const double *born_radii, double dielectric_in, double dielectric_out, double *egb,
                             double *dera, double *dgbdr, void *stream);
 
+/* Arithmetic peaks of GPU `device` measured by the library's own
+   throughput kernels (about 0.1 s): out[0] FP32 flop/s counting an FMA as
+   two, out[1] FP64 flop/s, out[2] ex2 special-function op/s, out[3] the
+   runtime's nominal SM clock (MHz).  The denominators of the pair stages'
+   roofline.  Returns 4, or -1 on error.  No counterpart in the reference. */
+int agbnp3_measure_peaks(int device, double *out, int n);
+
 #ifdef __cplusplus
 }
 #endif

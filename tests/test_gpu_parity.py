@@ -267,3 +267,26 @@ def test_capacity_regrowth(engine, monkeypatch):
         assert inst.stats()["error"] == 0
     finally:
         inst.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+def test_one_sided_pair_kernels(engine, monkeypatch, prec):
+    """The one-sided tiled GB pair kernels (AGBNP3_PAIR_TILED=1, each
+    ordered pair evaluated by its first atom) against the oracle, and in
+    FP64 against the default symmetric kernels."""
+    s, _ = load_golden("globule2000_hbmix")
+    q = O.oracle_eval(s)
+    base = A.Instance(s, precision=prec)
+    monkeypatch.setenv("AGBNP3_PAIR_TILED", "1")
+    inst = A.Instance(s, precision=prec)
+    try:
+        r = inst.ener()
+        check_vs_oracle(r, q, prec, "tiled")
+        if prec == A.PREC_FP64:
+            b = base.ener()
+            for k in ("egb", "evdw"):
+                assert abs(r[k] - b[k]) <= 1e-10 * max(abs(b[k]), 1.0)
+            assert rms_rel(r["dgbdr"], b["dgbdr"]) <= 1e-10
+    finally:
+        inst.close()
+        base.close()
