@@ -105,6 +105,7 @@ struct View {
   int *nl_c27, *nl_o27; /* near-list counts / offsets per (atom, neighbour cell) */
   int *nl_tmp, *nl_own; /* unsorted entries and their atom */
   int *ws_c27, *ws_o27, *ws_cand; /* water-site candidates per (site, cell) */
+  int *ws_srt;                    /* the same candidates in index order */
   int cap_wsc;
   double *acc_beta; /* descreening sums */
   /* Q4 tables as per-interval cubics in t = a/h - k, c0..c3 */
@@ -412,55 +413,79 @@ __device__ __forceinline__ void vol_terms(const View &v, int k, const Ov<R> &o, 
   dsurf = (double)((h3 * u1 + h4 * d2 / u1) / (R)v.r[k]);
 }
 
-/* order 2: candidates are the near-list pairs of each heavy atom */
+/* order 2: candidates are the near-list pairs, one thread per entry; the
+   kept flags are scanned in list order, so the records of an atom stay
+   contiguous and in its near-list order */
 template <typename R>
 __global__ void k_l2_count(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
-  AGB_GRID_STRIDE(g, v.natoms) {
-    int n = v.nl_count[g], o = v.nl_off[g], cnt = 0;
-    if (n > 0 && o + n <= v.cap_nl)
-      for (int k = 0; k < n; k++) {
-        Ov<R> ov = atom_pair<R>(v, (int)g, v.nl_list[o + k]);
-        if (kept(ov.gvolp)) cnt++;
-      }
-    v.lv_cnt[2][g] = cnt;
+  const int n = min(v.dc[DC_NL], v.cap_nl);
+  AGB_GRID_STRIDE(e, n) {
+    Ov<R> ov = atom_pair<R>(v, v.nl_own[e], v.nl_list[e]);
+    v.lv_cnt[2][e] = kept(ov.gvolp) ? 1 : 0;
   }
 }
 
-/* the records of one thread share their first parent: its sums stay in
-   registers and go out with one atomic each at the end */
+/* sum of a[0..1] over the run of consecutive lanes holding this lane's key;
+   returns whether this lane ends its run */
+__device__ __forceinline__ bool seg_scan2(double &a0, double &a1, int key) {
+  const int lane = threadIdx.x & 31;
+  int kp = __shfl_up_sync(0xffffffffu, key, 1);
+  int kn = __shfl_down_sync(0xffffffffu, key, 1);
+  unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || kp != key);
+  int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+  for (int o = 1; o < 32; o <<= 1) {
+    bool take = lane - o >= start;
+    double t0 = __shfl_up_sync(0xffffffffu, a0, o), t1 = __shfl_up_sync(0xffffffffu, a1, o);
+    if (take) {
+      a0 += t0;
+      a1 += t1;
+    }
+  }
+  return lane == 31 || kn != key;
+}
+
+/* warp-uniform loop over the entries; the first parent (the list's atom) is
+   shared by runs of consecutive entries and its sums are reduced in the
+   warp before the atomics */
 template <typename R>
 __global__ void k_l2_emit(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
-  AGB_GRID_STRIDE(g, v.natoms) {
-    int n = v.nl_count[g], o = v.nl_off[g];
-    if (n == 0 || o + n > v.cap_nl) continue;
-    int q = v.lv_off[2][g], qend = q + v.lv_cnt[2][g];
-    if (q == qend) continue;
-    if (qend > v.cap[2]) {
-      set_err(v, AGB_ERR_TREE_CAP);
-      continue;
+  const int n = min(v.dc[DC_NL], v.cap_nl);
+  const int c2 = v.cap[2], total = v.dc[DC_L0 + 2];
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long base = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n;
+       base += nwarps * 32) {
+    const int e = (int)base + lane;
+    int g = -1 - lane;
+    double dvg = 0.0, dsg = 0.0;
+    if (e < n && v.lv_cnt[2][e]) {
+      int q = v.lv_off[2][e];
+      g = v.nl_own[e];
+      int j = v.nl_list[e];
+      if (q < c2) {
+        int se = v.nl_off[g] + v.nl_count[g]; /* end of g's list */
+        int qend = se < n ? v.lv_off[2][se] : total;
+        Ov<R> ov = atom_pair<R>(v, g, j);
+        v.par[2][q] = g;
+        v.par[2][c2 + q] = j;
+        rec_put<R>(v, 2, q, ov);
+        v.gend[2][q] = qend;
+        double dv, ds;
+        vol_terms<R, 2>(v, g, ov, dvg, dsg);
+        vol_terms<R, 2>(v, j, ov, dv, ds);
+        atomicAdd(&v.volumep[j], dv);
+        atomicAdd(&v.surf[j], ds);
+      } else {
+        set_err(v, AGB_ERR_TREE_CAP);
+        g = -1 - lane;
+      }
     }
-    double svol = 0.0, ssurf = 0.0;
-    for (int k = 0; k < n; k++) {
-      int j = v.nl_list[o + k];
-      Ov<R> ov = atom_pair<R>(v, (int)g, j);
-      if (!kept(ov.gvolp)) continue;
-      v.par[2][q] = (int)g;
-      v.par[2][v.cap[2] + q] = j;
-      rec_put<R>(v, 2, q, ov);
-      v.gend[2][q] = qend;
-      double dv, ds;
-      vol_terms<R, 2>(v, (int)g, ov, dv, ds);
-      svol += dv;
-      ssurf += ds;
-      vol_terms<R, 2>(v, j, ov, dv, ds);
-      atomicAdd(&v.volumep[j], dv);
-      atomicAdd(&v.surf[j], ds);
-      q++;
+    if (seg_scan2(dvg, dsg, g) && g >= 0) {
+      atomicAdd(&v.volumep[g], dvg);
+      atomicAdd(&v.surf[g], dsg);
     }
-    atomicAdd(&v.volumep[g], svol);
-    atomicAdd(&v.surf[g], ssurf);
   }
 }
 
@@ -1528,54 +1553,86 @@ __global__ void k_ws_emit27(View v) {
 
 /* free volumes, HB energy and gradient (agbnp3_cpu_simd_kernels.c:
    2831-2933): the candidates of a site in heavy-atom index order, spe-
-   weighted overlaps subtracted until the free volume drops to 60% */
+   weighted overlaps subtracted until the free volume drops to 60%.  One
+   warp per site: the lanes rank-sort the candidates and evaluate their
+   overlaps 32 at a time; the subtraction itself then walks those 32 in
+   order (values broadcast from their lanes), so the free volume and the
+   point where it stops are those of the sequential loop. */
 template <typename R>
-__global__ void k_ws_free(View v) {
+__global__ void __launch_bounds__(128) k_ws_free(View v) {
+  const int lane = threadIdx.x & 31;
   const R *wpos = (const R *)v.wpos, *wd = (const R *)v.wdpos;
   const R vw = R(4.0 / 3.0 * C_PI * C_HBRAD * C_HBRAD * C_HBRAD);
   const R aw = R(C_KFC / (C_HBRAD * C_HBRAD));
-  AGB_GRID_STRIDE(w, v.nws) {
-    if (v.dc[DC_ERR] & AGB_ERR_WS_CAP) continue;
-    int o = v.ws_o27[27 * w], e = (w + 1 < v.nws) ? v.ws_o27[27 * (w + 1)] : v.dc[DC_WSC];
-    int *cand = v.ws_cand + o;
-    int nc = e - o;
-    for (int a = 1; a < nc; a++) { /* index order */
-      int h = cand[a], k = a;
-      while (k > 0 && cand[k - 1] > h) {
-        cand[k] = cand[k - 1];
-        k--;
+  const unsigned below = (1u << lane) - 1u;
+  if (v.dc[DC_ERR] & AGB_ERR_WS_CAP) return;
+  for (int w = blockIdx.x * 4 + (threadIdx.x >> 5); w < v.nws; w += gridDim.x * 4) {
+    const int o = v.ws_o27[27 * w], e = (w + 1 < v.nws) ? v.ws_o27[27 * (w + 1)] : v.dc[DC_WSC];
+    const int nc = e - o;
+    const int *cand = v.ws_cand + o;
+    int *srt = v.ws_srt + o;
+    for (int c = lane; c < nc; c += 32) { /* index order; ties keep list order */
+      int h = cand[c], rank = 0;
+      for (int c2 = 0; c2 < nc; c2++) {
+        int h2 = cand[c2];
+        rank += (h2 < h) || (h2 == h && c2 < c);
       }
-      cand[k] = h;
+      srt[rank] = h;
     }
+    __syncwarp();
     V3<R> p = {wpos[3 * w], wpos[3 * w + 1], wpos[3 * w + 2]};
-    double fv = (double)vw, cut = C_HBSWA0 * (double)vw;
+    const double cut = C_HBSWA0 * (double)vw;
+    double fv = (double)vw;
     int prev = v.ws_prev[w];
+    double spe_prev = prev >= 0 ? v.spe[prev] : 0.0;
     int np = 0;
-    for (int c = 0; c < nc; c++) {
-      if (!(fv > cut)) break;
-      int h = cand[c];
-      Ov<R> ov = ogauss<R>(aw, R(C_PFC), p.x, p.y, p.z, atom_alpha<R>(v, h), R(C_PFC), px<R>(v, h), py<R>(v, h),
-                           pz<R>(v, h));
-      if (!(ov.gvolp > R(0))) continue;
-      double s_used = v.compat ? (prev >= 0 ? v.spe[prev] : 0.0) : v.spe[h];
-      fv -= s_used * (double)ov.gvolp;
-      prev = h;
-      cand[np++] = h; /* processed overlaps, compacted in place */
+    bool done = false;
+    for (int c0 = 0; c0 < nc && !done; c0 += 32) {
+      const int c = c0 + lane;
+      int h = c < nc ? srt[c] : 0;
+      double g = 0.0, sh = 0.0;
+      if (c < nc) {
+        Ov<R> ov = ogauss<R>(aw, R(C_PFC), p.x, p.y, p.z, atom_alpha<R>(v, h), R(C_PFC), px<R>(v, h),
+                             py<R>(v, h), pz<R>(v, h));
+        if (ov.gvolp > R(0)) {
+          g = (double)ov.gvolp;
+          sh = v.spe[h];
+        }
+      }
+      unsigned proc = 0;
+      const int kend = min(32, nc - c0);
+      for (int k = 0; k < kend; k++) {
+        double gk = __shfl_sync(0xffffffffu, g, k), sk = __shfl_sync(0xffffffffu, sh, k);
+        if (!(fv > cut)) {
+          done = true;
+          break;
+        }
+        if (!(gk > 0.0)) continue;
+        fv -= (v.compat ? spe_prev : sk) * gk;
+        spe_prev = sk;
+        proc |= 1u << k;
+      }
+      __syncwarp();
+      if (proc & (1u << lane)) srt[np + __popc(proc & below)] = h; /* processed overlaps, compacted */
+      np += __popc(proc);
     }
+    __syncwarp();
     double spw = fv / (double)vw, fp, fpp;
     double sw = poly_switch<double>(spw, C_HBSWA, C_HBSWB, fp, fpp);
     double khb = v.ws_khb[w];
     double dhw = khb * fp / (double)vw;
-    v.ews[w] = khb * sw;
-    v.wsp[w] = spw;
+    if (lane == 0) {
+      v.ews[w] = khb * sw;
+      v.wsp[w] = spw;
+    }
     double jw[3] = {0, 0, 0};
-    for (int c = 0; c < np; c++) {
-      int h = cand[c];
+    for (int c = lane; c < np; c += 32) {
+      int h = srt[c];
       R ah = atom_alpha<R>(v, h);
       Ov<R> ov = ogauss<R>(aw, R(C_PFC), p.x, p.y, p.z, ah, R(C_PFC), px<R>(v, h), py<R>(v, h), pz<R>(v, h));
-      double sh = v.spe[h];
+      double shh = v.spe[h];
       double fi = -2.0 * (double)(ah * ov.gvol * ov.fp), fw = -2.0 * (double)(aw * ov.gvol * ov.fp);
-      double uu = -sh * dhw;
+      double uu = -shh * dhw;
       atomicAdd(&v.g_hb[3 * h], uu * fi * (double)(px<R>(v, h) - ov.cx));
       atomicAdd(&v.g_hb[3 * h + 1], uu * fi * (double)(py<R>(v, h) - ov.cy));
       atomicAdd(&v.g_hb[3 * h + 2], uu * fi * (double)(pz<R>(v, h) - ov.cz));
@@ -1584,15 +1641,18 @@ __global__ void k_ws_free(View v) {
       jw[1] += uu * fw * (double)(p.y - ov.cy);
       jw[2] += uu * fw * (double)(p.z - ov.cz);
     }
-    int npar = v.ws_nparent[w];
-    for (int q = 0; q < npar; q++) {
+    for (int off = 16; off > 0; off >>= 1)
+      for (int k = 0; k < 3; k++) jw[k] += __shfl_xor_sync(0xffffffffu, jw[k], off);
+    /* the site's gradient through its parents: lane 3q+j takes parent q, axis j */
+    const int npar = v.ws_nparent[w];
+    if (lane < 3 * npar) {
+      int q = lane / 3, j = lane % 3;
       int a = v.ws_parent[4 * w + q];
-      for (int j = 0; j < 3; j++) {
-        double t = 0.0;
-        for (int k = 0; k < 3; k++) t += jw[k] * (double)wd[(size_t)w * 36 + q * 9 + k * 3 + j];
-        atomicAdd(&v.g_hb[3 * a + j], t);
-      }
+      double t = 0.0;
+      for (int k = 0; k < 3; k++) t += jw[k] * (double)wd[(size_t)w * 36 + q * 9 + k * 3 + j];
+      atomicAdd(&v.g_hb[3 * a + j], t);
     }
+    __syncwarp();
   }
 }
 
@@ -1851,13 +1911,14 @@ static int tree_free(agb_dev *s) {
     s->v.rec[m] = NULL;
     s->v.gend[m] = NULL;
   }
-  for (int m = 3; m <= AGB_MAX_ORDER; m++) {
+  for (int m = 2; m <= AGB_MAX_ORDER; m++) {
     if (s->v.lv_cnt[m]) cudaFree(s->v.lv_cnt[m]);
     if (s->v.lv_off[m]) cudaFree(s->v.lv_off[m]);
     s->v.lv_cnt[m] = s->v.lv_off[m] = NULL;
   }
   if (s->v.ws_cand) cudaFree(s->v.ws_cand);
-  s->v.ws_cand = NULL;
+  if (s->v.ws_srt) cudaFree(s->v.ws_srt);
+  s->v.ws_cand = s->v.ws_srt = NULL;
   if (s->v.nl_list) cudaFree(s->v.nl_list);
   if (s->v.nl_d2) cudaFree(s->v.nl_d2);
   if (s->v.nl_tmp) cudaFree(s->v.nl_tmp);
@@ -1873,6 +1934,7 @@ static int tree_free(agb_dev *s) {
 static int tree_alloc(agb_dev *s) {
   size_t rsz = sizeof(double); /* records sized for the wider type */
   CK(cudaMalloc((void **)&s->v.ws_cand, sizeof(int) * (size_t)s->cap_wsc));
+  CK(cudaMalloc((void **)&s->v.ws_srt, sizeof(int) * (size_t)s->cap_wsc));
   s->v.cap_wsc = s->cap_wsc;
   CK(cudaMalloc((void **)&s->v.nl_list, sizeof(int) * (size_t)s->cap_nl));
   CK(cudaMalloc((void **)&s->v.nl_d2, sizeof(float) * (size_t)s->cap_nl));
@@ -1886,6 +1948,9 @@ static int tree_alloc(agb_dev *s) {
     if (s->cap[m] > maxcap) maxcap = s->cap[m];
     s->v.cap[m] = s->cap[m];
   }
+  /* order 2: one kept flag / offset per near-list entry */
+  CK(cudaMalloc((void **)&s->v.lv_cnt[2], sizeof(int) * (size_t)s->cap_nl));
+  CK(cudaMalloc((void **)&s->v.lv_off[2], sizeof(int) * (size_t)s->cap_nl));
   for (int m = 3; m <= AGB_MAX_ORDER; m++) {
     /* one count / offset per generating overlap of order m-1 */
     CK(cudaMalloc((void **)&s->v.lv_cnt[m], sizeof(int) * (size_t)s->cap[m - 1]));
@@ -2117,8 +2182,6 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   DALLOC(v.nl_o27, 27 * N, int);
   DALLOC(v.ws_c27, 27 * (NW > 0 ? NW : 1), int);
   DALLOC(v.ws_o27, 27 * (NW > 0 ? NW : 1), int);
-  DALLOC(v.lv_cnt[2], N, int);
-  DALLOC(v.lv_off[2], N, int);
   DALLOC(v.dc, DC_SIZE, int);
   double **dbl[] = {&v.volumep, &v.surf, &v.surf_f, &v.sp, &v.spe, &v.psvol, &v.gammap, &v.bfil, &v.bder,
                     &v.br, &v.brw, &v.dera, &v.q2ab, &v.abrw, &v.deru, &v.derv, &v.derh, &v.derus, &v.dervs,
@@ -2278,9 +2341,9 @@ static void launch_all(agb_dev *s) {
   AGB_LAUNCH(k_nl_rank, nblocks(s->cap_nl), BLK, st, v);
   nl += 6 + 6;
   stage_mark(s, 2);
-  AGB_LAUNCH(k_l2_count<R>, nblocks(N), BLK, st, v);
-  agb_scan_excl(v.lv_cnt[2], v.lv_off[2], v.dc + DC_N, v.dc + DC_L0 + 2, N, s->scan_scratch, st);
-  AGB_LAUNCH(k_l2_emit<R>, nblocks(N), BLK, st, v);
+  AGB_LAUNCH(k_l2_count<R>, nblocks(s->cap_nl), BLK, st, v);
+  agb_scan_excl(v.lv_cnt[2], v.lv_off[2], v.dc + DC_NL, v.dc + DC_L0 + 2, s->cap_nl, s->scan_scratch, st);
+  AGB_LAUNCH(k_l2_emit<R>, nblocks(s->cap_nl), BLK, st, v);
   nl += 2 + 3;
   for (int m = 3; m <= AGB_MAX_ORDER; m++) {
     int g = nblocks(v.cap[m - 1]);
@@ -2327,7 +2390,7 @@ static void launch_all(agb_dev *s) {
     AGB_LAUNCH(k_ws_count27<R>, nblocks(27LL * s->nws), BLK, st, v);
     agb_scan_excl(v.ws_c27, v.ws_o27, v.dc + DC_W27, v.dc + DC_WSC, 27 * s->nws, s->scan_scratch, st);
     AGB_LAUNCH(k_ws_emit27<R>, nblocks(27LL * s->nws), BLK, st, v);
-    AGB_LAUNCH(k_ws_free<R>, nblocks(s->nws), BLK, st, v);
+    AGB_LAUNCH(k_ws_free<R>, sym_grid(s->nws), 128, st, v);
     nl += 4 + 3;
   }
   stage_mark(s, 8);
