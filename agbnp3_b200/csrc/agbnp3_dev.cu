@@ -83,7 +83,9 @@ struct View {
   f4 *pos;
   double *pxd, *pyd, *pzd;
   int *atom_cell, *atom_bucket;
-  int *bucket_count, *bucket_start, *bucket_cursor, *cell_atoms;
+  int *bucket_count, *bucket_start, *bucket_cursor;
+  f4 *cell_pos;  /* per bucket slot: the atom's position and radius */
+  int2 *cell_id; /* per bucket slot: the atom and its packed cell */
   int *nl_count, *nl_off, *nl_list;
   float *nl_d2;
   int cap_nl;
@@ -238,6 +240,12 @@ __device__ __forceinline__ int cell_hash(int cx, int cy, int cz, int mask) {
   return (int)(h & (unsigned)mask);
 }
 
+/* 10 bits per axis: the 27 cells around any cell have distinct keys, and a
+   far cell sharing a key holds only atoms beyond every cutoff */
+__device__ __forceinline__ int cell_key(int cx, int cy, int cz) {
+  return (cx & 1023) | ((cy & 1023) << 10) | ((cz & 1023) << 20);
+}
+
 __device__ __forceinline__ void cell_of(float x, float y, float z, float inv, int &cx, int &cy, int &cz) {
   cx = (int)floorf(x * inv);
   cy = (int)floorf(y * inv);
@@ -267,8 +275,9 @@ __global__ void k_cell_fill(View v) {
     if (g >= v.inst_begin[I] + v.inst_nheavy[I]) continue;
     int b = v.atom_bucket[g];
     /* slot order inside a bucket is arbitrary; every consumer sorts */
-    int s = atomicAdd(&v.bucket_cursor[b], 1);
-    v.cell_atoms[v.bucket_start[b] + s] = (int)g;
+    int s = v.bucket_start[b] + atomicAdd(&v.bucket_cursor[b], 1);
+    v.cell_pos[s] = v.pos[g];
+    v.cell_id[s] = make_int2((int)g, cell_key(v.atom_cell[3 * g], v.atom_cell[3 * g + 1], v.atom_cell[3 * g + 2]));
   }
 }
 
@@ -281,15 +290,17 @@ __device__ __forceinline__ bool near_test(const f4 &a, const f4 &b, float &d2) {
   return d2 < __fmul_rn(u, u);
 }
 
-/* the heavy atoms of instance I in cell (ax, ay, az): fn(j) once each */
+/* the heavy atoms of instance I in cell (ax, ay, az): fn(j, position of j)
+   once each; a bucket's slots are contiguous records */
 template <typename Fn>
 __device__ __forceinline__ void for_cell(const View &v, int I, int ax, int ay, int az, Fn fn) {
   int b = v.bucket_begin[I] + cell_hash(ax, ay, az, v.bucket_mask[I]);
   int s0 = v.bucket_start[b], s1 = s0 + v.bucket_count[b];
+  const int key = cell_key(ax, ay, az);
   for (int s = s0; s < s1; s++) {
-    int j = v.cell_atoms[s];
-    if (v.atom_cell[3 * j] != ax || v.atom_cell[3 * j + 1] != ay || v.atom_cell[3 * j + 2] != az) continue;
-    fn(j);
+    int2 id = v.cell_id[s];
+    f4 p = v.cell_pos[s];
+    if (id.y == key) fn(id.x, p);
   }
 }
 
@@ -302,9 +313,9 @@ __global__ void k_nl_count27(View v) {
     if (g < v.inst_begin[I] + v.inst_nheavy[I]) {
       f4 a = v.pos[g];
       for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
-               v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j) {
+               v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j, const f4 &b) {
                  float d2;
-                 if (j > g && near_test(a, v.pos[j], d2)) cnt++;
+                 if (j > g && near_test(a, b, d2)) cnt++;
                });
     }
     v.nl_c27[q] = cnt;
@@ -325,9 +336,9 @@ __global__ void k_nl_emit27(View v) {
     f4 a = v.pos[g];
     int m = 0;
     for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
-             v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j) {
+             v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j, const f4 &b) {
                float d2;
-               if (j > g && near_test(a, v.pos[j], d2) && m < n) {
+               if (j > g && near_test(a, b, d2) && m < n) {
                  v.nl_tmp[o + m] = j;
                  v.nl_d2[o + m] = d2;
                  v.nl_own[o + m] = g;
@@ -1522,9 +1533,20 @@ __device__ __forceinline__ int ws_cell_scan(const View &v, int w, int c, int *ou
   int cx, cy, cz;
   cell_of((float)px_, (float)py_, (float)pz_, inv, cx, cy, cz);
   int m = 0;
-  for_cell(v, I, cx + c % 3 - 1, cy + (c / 3) % 3 - 1, cz + c / 9 - 1, [&](int h) {
-    R dx = px<R>(v, h) - px_, dy = py<R>(v, h) - py_, dz = pz<R>(v, h) - pz_;
-    R u = ((R)v.r[h] + R(C_HBRAD)) * R(1.6);
+  for_cell(v, I, cx + c % 3 - 1, cy + (c / 3) % 3 - 1, cz + c / 9 - 1, [&](int h, const f4 &b) {
+    R dx, dy, dz, rh;
+    if constexpr (sizeof(R) == sizeof(float)) { /* the slot record holds the float position and radius */
+      dx = b.x - px_;
+      dy = b.y - py_;
+      dz = b.z - pz_;
+      rh = b.w;
+    } else {
+      dx = px<R>(v, h) - px_;
+      dy = py<R>(v, h) - py_;
+      dz = pz<R>(v, h) - pz_;
+      rh = (R)v.r[h];
+    }
+    R u = (rh + R(C_HBRAD)) * R(1.6);
     if (dx * dx + dy * dy + dz * dz < u * u) {
       if (out && m < cap) out[m] = h;
       m++;
@@ -2175,7 +2197,8 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   DALLOC(v.bucket_count, nb, int);
   DALLOC(v.bucket_start, nb, int);
   DALLOC(v.bucket_cursor, nb, int);
-  DALLOC(v.cell_atoms, N, int);
+  DALLOC(v.cell_pos, N, f4);
+  DALLOC(v.cell_id, N, int2);
   DALLOC(v.nl_count, N, int);
   DALLOC(v.nl_off, N, int);
   DALLOC(v.nl_c27, 27 * N, int);
