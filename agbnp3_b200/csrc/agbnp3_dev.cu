@@ -1037,7 +1037,55 @@ __device__ __forceinline__ T rot1(T x) {
 }
 
 /* agb: GB pair energy, constant-B gradient, A_i (agbnp3_cpu_simd_kernels.c:
-   66-151, 329-460) */
+   66-151, 329-460).  Interior j tiles (all valid, after the i block) skip
+   the per-pair index tests. */
+template <typename R>
+struct AgbI {
+  int ia[2];
+  R x[2], y[2], z[2], q[2], b[2], c[2];
+};
+template <typename R>
+struct AgbJ {
+  R x, y, z, q, b, bi;
+  R gx, gy, gz, at;
+};
+template <typename R>
+struct AgbP {
+  R e[2], gx[2], gy[2], gz[2], at[2];
+};
+
+template <typename R, bool FULL>
+__device__ __forceinline__ void agb_tile(const AgbI<R> &I, AgbJ<R> &J, AgbP<R> &P, int lane, int j0, int a1) {
+  for (int r = 0; r < 32; r++) {
+    if (r > 0) {
+      J.x = rot1(J.x); J.y = rot1(J.y); J.z = rot1(J.z);
+      J.q = rot1(J.q); J.b = rot1(J.b); J.bi = rot1(J.bi);
+    }
+    const int jr = j0 + ((lane + r) & 31);
+    const bool jok = FULL || jr < a1;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      R dx = J.x - I.x[u], dy = J.y - I.y[u], dz = J.z - I.z[u];
+      R d2 = dx * dx + dy * dy + dz * dz;
+      if (!((FULL || (jok && I.ia[u] < jr)) && d2 > R(0))) continue; /* coincident atoms are skipped */
+      R bb = I.b[u] * J.b;
+      R et = GbExp<R>::ex(I.c[u] * J.bi * d2);
+      R f = m_rsqrt(d2 + bb * et);
+      R qq = I.q[u] * J.q;
+      R qf3 = qq * f * f * f;
+      P.e[u] += qq * f;
+      R mw = (R(1) - R(0.25) * et) * qf3;
+      R gx = mw * dx, gy = mw * dy, gz = mw * dz;
+      P.gx[u] += gx; P.gy[u] += gy; P.gz[u] += gz;
+      J.gx -= gx; J.gy -= gy; J.gz -= gz;
+      R at = (bb + R(0.25) * d2) * et * qf3;
+      P.at[u] += at;
+      J.at += at;
+    }
+    J.gx = rot1(J.gx); J.gy = rot1(J.gy); J.gz = rot1(J.gz); J.at = rot1(J.at);
+  }
+}
+
 template <typename R>
 __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict__ items, int nitems) {
   const int lane = threadIdx.x & 31;
@@ -1047,79 +1095,59 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
   for (int it = blockIdx.x * 4 + (threadIdx.x >> 5); it < nitems; it += gridDim.x * 4) {
     int4 w = items[it]; /* instance, first atom of the i block, first atom of the j run, j tiles */
     const int a1 = v.inst_begin[w.x + 1];
-    int ia[2];
-    R xi[2], yi[2], zi[2], qi[2], bi[2], ci[2];
+    const double w2 = 2.0 * v.inst_df[w.x];
+    AgbI<R> I;
     double se[2], sgx[2], sgy[2], sgz[2], sat[2];
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-      ia[u] = w.y + 32 * u + lane;
-      bool ok = ia[u] < a1;
-      xi[u] = ok ? X[ia[u]] : R(0);
-      yi[u] = ok ? Y[ia[u]] : R(0);
-      zi[u] = ok ? Z[ia[u]] : R(0);
-      qi[u] = ok ? Q[ia[u]] : R(0);
-      bi[u] = ok ? Bv[ia[u]] : R(1);
-      ci[u] = ok ? GbExp<R>::scale() * BI[ia[u]] : R(0);
-      if (!ok) ia[u] = INT_MAX; /* no valid partner: i < j never holds */
+      int i = w.y + 32 * u + lane;
+      bool ok = i < a1;
+      I.x[u] = ok ? X[i] : R(0);
+      I.y[u] = ok ? Y[i] : R(0);
+      I.z[u] = ok ? Z[i] : R(0);
+      I.q[u] = ok ? Q[i] : R(0);
+      I.b[u] = ok ? Bv[i] : R(1);
+      I.c[u] = ok ? GbExp<R>::scale() * BI[i] : R(0);
+      I.ia[u] = ok ? i : INT_MAX; /* no valid partner: i < j never holds */
       se[u] = sgx[u] = sgy[u] = sgz[u] = sat[u] = 0.0;
     }
     for (int k = 0; k < w.w; k++) {
       const int j0 = w.z + 32 * k;
-      int j = j0 + lane;
-      bool vj = j < a1;
-      R xj = vj ? X[j] : R(0), yj = vj ? Y[j] : R(0), zj = vj ? Z[j] : R(0);
-      R qj = vj ? Q[j] : R(0), bj = vj ? Bv[j] : R(1), bij = vj ? BI[j] : R(0);
-      R jgx = 0, jgy = 0, jgz = 0, jat = 0;
-      R pe[2] = {0, 0}, pgx[2] = {0, 0}, pgy[2] = {0, 0}, pgz[2] = {0, 0}, pat[2] = {0, 0};
-      for (int r = 0; r < 32; r++) {
-        if (r > 0) {
-          xj = rot1(xj); yj = rot1(yj); zj = rot1(zj);
-          qj = rot1(qj); bj = rot1(bj); bij = rot1(bij);
-        }
-        const int jr = j0 + ((lane + r) & 31);
-        const bool jok = jr < a1;
+      const int j = j0 + lane;
+      const bool vj = j < a1;
+      AgbJ<R> J;
+      J.x = vj ? X[j] : R(0);
+      J.y = vj ? Y[j] : R(0);
+      J.z = vj ? Z[j] : R(0);
+      J.q = vj ? Q[j] : R(0);
+      J.b = vj ? Bv[j] : R(1);
+      J.bi = vj ? BI[j] : R(0);
+      J.gx = J.gy = J.gz = J.at = R(0);
+      AgbP<R> P;
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-          R dx = xj - xi[u], dy = yj - yi[u], dz = zj - zi[u];
-          R d2 = dx * dx + dy * dy + dz * dz;
-          if (jok && ia[u] < jr && d2 > R(0)) { /* coincident atoms are skipped */
-            R bb = bi[u] * bj;
-            R et = GbExp<R>::ex(ci[u] * bij * d2);
-            R f = m_rsqrt(d2 + bb * et);
-            R qq = qi[u] * qj;
-            R qf3 = qq * f * f * f;
-            pe[u] += qq * f;
-            R mw = (R(1) - R(0.25) * et) * qf3;
-            R gx = mw * dx, gy = mw * dy, gz = mw * dz;
-            pgx[u] += gx; pgy[u] += gy; pgz[u] += gz;
-            jgx -= gx; jgy -= gy; jgz -= gz;
-            R at = (bb + R(0.25) * d2) * et * qf3;
-            pat[u] += at;
-            jat += at;
-          }
-        }
-        jgx = rot1(jgx); jgy = rot1(jgy); jgz = rot1(jgz); jat = rot1(jat);
-      }
+      for (int u = 0; u < 2; u++) P.e[u] = P.gx[u] = P.gy[u] = P.gz[u] = P.at[u] = R(0);
+      if (w.y + 64 <= a1 && j0 >= w.y + 64 && j0 + 32 <= a1) /* warp-uniform */
+        agb_tile<R, true>(I, J, P, lane, j0, a1);
+      else
+        agb_tile<R, false>(I, J, P, lane, j0, a1);
       if (vj) {
-        double w2 = 2.0 * v.inst_df[w.x];
-        atomicAdd(&v.g_gb[3 * j], w2 * (double)jgx);
-        atomicAdd(&v.g_gb[3 * j + 1], w2 * (double)jgy);
-        atomicAdd(&v.g_gb[3 * j + 2], w2 * (double)jgz);
-        atomicAdd(&v.dera[j], (double)jat);
+        atomicAdd(&v.g_gb[3 * j], w2 * (double)J.gx);
+        atomicAdd(&v.g_gb[3 * j + 1], w2 * (double)J.gy);
+        atomicAdd(&v.g_gb[3 * j + 2], w2 * (double)J.gz);
+        atomicAdd(&v.dera[j], (double)J.at);
       }
 #pragma unroll
       for (int u = 0; u < 2; u++) {
-        se[u] += (double)pe[u];
-        sgx[u] += (double)pgx[u];
-        sgy[u] += (double)pgy[u];
-        sgz[u] += (double)pgz[u];
-        sat[u] += (double)pat[u];
+        se[u] += (double)P.e[u];
+        sgx[u] += (double)P.gx[u];
+        sgy[u] += (double)P.gy[u];
+        sgz[u] += (double)P.gz[u];
+        sat[u] += (double)P.at[u];
       }
     }
-    const double w2 = 2.0 * v.inst_df[w.x];
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-      int i = ia[u];
+      int i = I.ia[u];
       if (i >= a1) continue;
       atomicAdd(&v.eatom[N + i], C_TOKCAL * w2 * se[u]);
       atomicAdd(&v.g_gb[3 * i], w2 * sgx[u]);
@@ -1131,7 +1159,106 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
 }
 
 /* gbders: both descreening directions of every unordered pair with a heavy
-   atom, pair forces, U and V (agbnp3_cpu_simd_kernels.c:681-904) */
+   atom, pair forces, U and V (agbnp3_cpu_simd_kernels.c:681-904).  After
+   the heavy-first ordering almost every j tile is interior: all 32 atoms
+   valid, after the i block, and all heavy (both directions) or all
+   hydrogens (only "j descreened by i"); those tiles run a rotation loop
+   without per-pair flags, the table-range test done by selects. */
+enum { GBD_GEN = 0, GBD_HH = 1, GBD_HX = 2 };
+
+template <typename R>
+struct GbdI { /* a lane's two i atoms */
+  int ia[2], ti[2];
+  bool hi[2];
+  R x[2], y[2], z[2], rh[2], ri[2], sp[2], q2[2], ab[2];
+};
+template <typename R>
+struct GbdJ { /* the j atom a lane holds in a rotation step, and its sums */
+  R x, y, z, rh, ri, sp, q2, ab;
+  int t;
+  R U, V, fx, fy, fz, vx, vy, vz;
+};
+template <typename R>
+struct GbdP { /* i-side sums over one j tile */
+  R U[2], V[2], fx[2], fy[2], fz[2], vx[2], vy[2], vz[2];
+};
+
+/* Q4 of the atom of type `td` descreened by an atom of 1/(R h) rhs and
+   1/R ris at distance d, and its derivative factor dQ4/dd * ris^2 scale */
+template <typename R, bool SEL>
+__device__ __forceinline__ bool gbd_q4(const typename Tab<R>::T *tv, int slot, R d, R rhs, R ris, R kref, R hinv,
+                                       R &q, R &dq) {
+  R xh = d * rhs;
+  bool in = xh < R(AGB_NA - 1);
+  if (SEL) {
+    R fp;
+    R f = spline_d<R>(tv, slot, in ? xh : R(0), kref, fp);
+    q = in ? f * ris : R(0);
+    dq = in ? fp * hinv * ris * ris : R(0);
+    return true;
+  }
+  if (!in) return false;
+  R fp;
+  R f = spline_d<R>(tv, slot, xh, kref, fp);
+  q = f * ris;
+  dq = fp * hinv * ris * ris;
+  return true;
+}
+
+template <typename R, int MODE>
+__device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &P, int lane, int j0, int a1, int hh,
+                                         const typename Tab<R>::T *tv, R kref, R hinv, int nt) {
+  for (int r = 0; r < 32; r++) {
+    if (r > 0) {
+      J.x = rot1(J.x); J.y = rot1(J.y); J.z = rot1(J.z);
+      J.rh = rot1(J.rh); J.ri = rot1(J.ri); J.sp = rot1(J.sp);
+      J.q2 = rot1(J.q2); J.ab = rot1(J.ab); J.t = rot1(J.t);
+    }
+    const int jr = j0 + ((lane + r) & 31);
+    const bool jok = MODE != GBD_GEN || jr < a1;
+    const bool hj = MODE == GBD_HH || (MODE == GBD_GEN && jr < hh);
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const bool hiu = MODE != GBD_GEN || I.hi[u];
+      R dx = J.x - I.x[u], dy = J.y - I.y[u], dz = J.z - I.z[u];
+      R d2 = dx * dx + dy * dy + dz * dz;
+      if (MODE == GBD_GEN) {
+        if (!(jok && I.ia[u] < jr && (hiu || hj) && d2 > R(0))) continue;
+      } else if (!(d2 > R(0))) {
+        continue; /* coincident atoms */
+      }
+      R id = m_rsqrt(d2);
+      R d = d2 * id;
+      R ht = R(0), ut = R(0), q, dq;
+      if (hiu && gbd_q4<R, MODE != GBD_GEN>(tv, J.t * nt + I.ti[u], d, I.rh[u], I.ri[u], kref, hinv, q, dq)) {
+        /* j descreened by i: table (type j, type i), radius of i */
+        P.U[u] += J.q2 * q;
+        P.V[u] += J.ab * q;
+        ht += J.q2 * dq * I.sp[u];
+        ut += J.ab * dq * I.sp[u];
+      }
+      if (hj && gbd_q4<R, MODE != GBD_GEN>(tv, I.ti[u] * nt + J.t, d, J.rh, J.ri, kref, hinv, q, dq)) {
+        /* i descreened by j: table (type i, type j), radius of j */
+        J.U += I.q2[u] * q;
+        J.V += I.ab[u] * q;
+        ht += I.q2[u] * dq * J.sp;
+        ut += I.ab[u] * dq * J.sp;
+      }
+      ht *= id;
+      ut *= id;
+      R fx = ht * dx, fy = ht * dy, fz = ht * dz;
+      R ux = ut * dx, uy = ut * dy, uz = ut * dz;
+      P.fx[u] += fx; P.fy[u] += fy; P.fz[u] += fz;
+      P.vx[u] += ux; P.vy[u] += uy; P.vz[u] += uz;
+      J.fx -= fx; J.fy -= fy; J.fz -= fz;
+      J.vx -= ux; J.vy -= uy; J.vz -= uz;
+    }
+    J.U = rot1(J.U); J.V = rot1(J.V);
+    J.fx = rot1(J.fx); J.fy = rot1(J.fy); J.fz = rot1(J.fz);
+    J.vx = rot1(J.vx); J.vy = rot1(J.vy); J.vz = rot1(J.vz);
+  }
+}
+
 template <typename R>
 __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restrict__ items, int nitems) {
   const int lane = threadIdx.x & 31;
@@ -1141,123 +1268,84 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
   const typename Tab<R>::T *tv = Tab<R>::val(v);
   const R kref = v.compat ? R(1) : R(0), hinv = R((AGB_NA - 1) / C_AMAX);
   const int nt = v.ntypes;
+  const double f4p = 1.0 / (4.0 * C_PI);
   for (int it = blockIdx.x * 4 + (threadIdx.x >> 5); it < nitems; it += gridDim.x * 4) {
     int4 w = items[it];
     const int a0 = v.inst_begin[w.x], hh = a0 + v.inst_nheavy[w.x], a1 = v.inst_begin[w.x + 1];
-    int ia[2], ti[2];
-    bool hi[2];
-    R xi[2], yi[2], zi[2], rhi[2], rii[2], spi[2], q2i[2], abi[2];
+    const double kg = f4p * v.inst_df[w.x];
+    GbdI<R> I;
     double sU[2], sV[2], sfx[2], sfy[2], sfz[2], svx[2], svy[2], svz[2];
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       int i = w.y + 32 * u + lane;
       bool ok = i < a1;
-      hi[u] = i < hh;
-      xi[u] = ok ? X[i] : R(0);
-      yi[u] = ok ? Y[i] : R(0);
-      zi[u] = ok ? Z[i] : R(0);
-      rhi[u] = ok ? RH[i] : R(0);
-      rii[u] = ok ? RI[i] : R(0);
-      spi[u] = ok ? SP[i] : R(0);
-      q2i[u] = ok ? Q2[i] : R(0);
-      abi[u] = ok ? AB[i] : R(0);
-      ti[u] = ok ? v.rtype[i] : 0;
-      ia[u] = ok ? i : INT_MAX; /* no valid partner: i < j never holds */
+      I.hi[u] = i < hh;
+      I.x[u] = ok ? X[i] : R(0);
+      I.y[u] = ok ? Y[i] : R(0);
+      I.z[u] = ok ? Z[i] : R(0);
+      I.rh[u] = ok ? RH[i] : R(0);
+      I.ri[u] = ok ? RI[i] : R(0);
+      I.sp[u] = ok ? SP[i] : R(0);
+      I.q2[u] = ok ? Q2[i] : R(0);
+      I.ab[u] = ok ? AB[i] : R(0);
+      I.ti[u] = ok ? v.rtype[i] : 0;
+      I.ia[u] = ok ? i : INT_MAX; /* no valid partner: i < j never holds */
       sU[u] = sV[u] = sfx[u] = sfy[u] = sfz[u] = svx[u] = svy[u] = svz[u] = 0.0;
     }
+    const bool iheavy = w.y + 64 <= hh; /* both i tiles complete and heavy */
     for (int k = 0; k < w.w; k++) {
       const int j0 = w.z + 32 * k;
-      int j = j0 + lane;
-      bool vj = j < a1;
-      R xj = vj ? X[j] : R(0), yj = vj ? Y[j] : R(0), zj = vj ? Z[j] : R(0);
-      R rhj = vj ? RH[j] : R(0), rij = vj ? RI[j] : R(0), spj = vj ? SP[j] : R(0);
-      R q2j = vj ? Q2[j] : R(0), abj = vj ? AB[j] : R(0);
-      int tj = vj ? v.rtype[j] : 0;
-      R jU = 0, jV = 0, jfx = 0, jfy = 0, jfz = 0, jvx = 0, jvy = 0, jvz = 0;
-      R pU[2] = {0, 0}, pV[2] = {0, 0}, pfx[2] = {0, 0}, pfy[2] = {0, 0}, pfz[2] = {0, 0};
-      R pvx[2] = {0, 0}, pvy[2] = {0, 0}, pvz[2] = {0, 0};
-      for (int r = 0; r < 32; r++) {
-        if (r > 0) {
-          xj = rot1(xj); yj = rot1(yj); zj = rot1(zj);
-          rhj = rot1(rhj); rij = rot1(rij); spj = rot1(spj);
-          q2j = rot1(q2j); abj = rot1(abj); tj = rot1(tj);
-        }
-        const int jr = j0 + ((lane + r) & 31);
-        const bool jok = jr < a1, hj = jr < hh;
+      const int j = j0 + lane;
+      const bool vj = j < a1;
+      GbdJ<R> J;
+      J.x = vj ? X[j] : R(0);
+      J.y = vj ? Y[j] : R(0);
+      J.z = vj ? Z[j] : R(0);
+      J.rh = vj ? RH[j] : R(0);
+      J.ri = vj ? RI[j] : R(0);
+      J.sp = vj ? SP[j] : R(0);
+      J.q2 = vj ? Q2[j] : R(0);
+      J.ab = vj ? AB[j] : R(0);
+      J.t = vj ? v.rtype[j] : 0;
+      J.U = J.V = J.fx = J.fy = J.fz = J.vx = J.vy = J.vz = R(0);
+      GbdP<R> P;
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-          R dx = xj - xi[u], dy = yj - yi[u], dz = zj - zi[u];
-          R d2 = dx * dx + dy * dy + dz * dz;
-          if (!(jok && ia[u] < jr && (hi[u] || hj) && d2 > R(0))) continue;
-          R id = m_rsqrt(d2);
-          R d = d2 * id;
-          R ht = R(0), ut = R(0);
-          if (hi[u]) { /* j descreened by i: table (type j, type i), radius of i */
-            R xh = d * rhi[u];
-            if (xh < R(AGB_NA - 1)) {
-              R fp;
-              R f = spline_d<R>(tv, tj * nt + ti[u], xh, kref, fp);
-              R q = f * rii[u], dq = fp * hinv * rii[u] * rii[u];
-              pU[u] += q2j * q;
-              pV[u] += abj * q;
-              ht += q2j * dq * spi[u];
-              ut += abj * dq * spi[u];
-            }
-          }
-          if (hj) { /* i descreened by j: table (type i, type j), radius of j */
-            R xh = d * rhj;
-            if (xh < R(AGB_NA - 1)) {
-              R fp;
-              R f = spline_d<R>(tv, ti[u] * nt + tj, xh, kref, fp);
-              R q = f * rij, dq = fp * hinv * rij * rij;
-              jU += q2i[u] * q;
-              jV += abi[u] * q;
-              ht += q2i[u] * dq * spj;
-              ut += abi[u] * dq * spj;
-            }
-          }
-          ht *= id;
-          ut *= id;
-          R fx = ht * dx, fy = ht * dy, fz = ht * dz;
-          R ux = ut * dx, uy = ut * dy, uz = ut * dz;
-          pfx[u] += fx; pfy[u] += fy; pfz[u] += fz;
-          pvx[u] += ux; pvy[u] += uy; pvz[u] += uz;
-          jfx -= fx; jfy -= fy; jfz -= fz;
-          jvx -= ux; jvy -= uy; jvz -= uz;
-        }
-        jU = rot1(jU); jV = rot1(jV);
-        jfx = rot1(jfx); jfy = rot1(jfy); jfz = rot1(jfz);
-        jvx = rot1(jvx); jvy = rot1(jvy); jvz = rot1(jvz);
-      }
-      const double f4p = 1.0 / (4.0 * C_PI), kg = f4p * v.inst_df[w.x];
+      for (int u = 0; u < 2; u++) P.U[u] = P.V[u] = P.fx[u] = P.fy[u] = P.fz[u] = P.vx[u] = P.vy[u] = P.vz[u] = R(0);
+      /* warp-uniform tile class */
+      const bool interior = iheavy && j0 >= w.y + 64;
+      if (interior && j0 + 32 <= hh)
+        gbd_tile<R, GBD_HH>(I, J, P, lane, j0, a1, hh, tv, kref, hinv, nt);
+      else if (interior && j0 >= hh && j0 + 32 <= a1)
+        gbd_tile<R, GBD_HX>(I, J, P, lane, j0, a1, hh, tv, kref, hinv, nt);
+      else
+        gbd_tile<R, GBD_GEN>(I, J, P, lane, j0, a1, hh, tv, kref, hinv, nt);
       if (vj) {
-        atomicAdd(&v.g_gb[3 * j], kg * (double)jfx);
-        atomicAdd(&v.g_gb[3 * j + 1], kg * (double)jfy);
-        atomicAdd(&v.g_gb[3 * j + 2], kg * (double)jfz);
-        atomicAdd(&v.g_vw[3 * j], f4p * (double)jvx);
-        atomicAdd(&v.g_vw[3 * j + 1], f4p * (double)jvy);
-        atomicAdd(&v.g_vw[3 * j + 2], f4p * (double)jvz);
+        atomicAdd(&v.g_gb[3 * j], kg * (double)J.fx);
+        atomicAdd(&v.g_gb[3 * j + 1], kg * (double)J.fy);
+        atomicAdd(&v.g_gb[3 * j + 2], kg * (double)J.fz);
+        atomicAdd(&v.g_vw[3 * j], f4p * (double)J.vx);
+        atomicAdd(&v.g_vw[3 * j + 1], f4p * (double)J.vy);
+        atomicAdd(&v.g_vw[3 * j + 2], f4p * (double)J.vz);
         if (j < hh) {
-          atomicAdd(&v.deru[j], (double)jU);
-          atomicAdd(&v.derv[j], (double)jV);
+          atomicAdd(&v.deru[j], (double)J.U);
+          atomicAdd(&v.derv[j], (double)J.V);
         }
       }
 #pragma unroll
       for (int u = 0; u < 2; u++) {
-        sU[u] += (double)pU[u];
-        sV[u] += (double)pV[u];
-        sfx[u] += (double)pfx[u];
-        sfy[u] += (double)pfy[u];
-        sfz[u] += (double)pfz[u];
-        svx[u] += (double)pvx[u];
-        svy[u] += (double)pvy[u];
-        svz[u] += (double)pvz[u];
+        sU[u] += (double)P.U[u];
+        sV[u] += (double)P.V[u];
+        sfx[u] += (double)P.fx[u];
+        sfy[u] += (double)P.fy[u];
+        sfz[u] += (double)P.fz[u];
+        svx[u] += (double)P.vx[u];
+        svy[u] += (double)P.vy[u];
+        svz[u] += (double)P.vz[u];
       }
     }
-    const double f4p = 1.0 / (4.0 * C_PI), kg = f4p * v.inst_df[w.x];
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-      int i = ia[u];
+      int i = I.ia[u];
       if (i >= a1) continue;
       atomicAdd(&v.g_gb[3 * i], kg * sfx[u]);
       atomicAdd(&v.g_gb[3 * i + 1], kg * sfy[u]);
@@ -1265,7 +1353,7 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       atomicAdd(&v.g_vw[3 * i], f4p * svx[u]);
       atomicAdd(&v.g_vw[3 * i + 1], f4p * svy[u]);
       atomicAdd(&v.g_vw[3 * i + 2], f4p * svz[u]);
-      if (hi[u]) {
+      if (I.hi[u]) {
         atomicAdd(&v.deru[i], sU[u]);
         atomicAdd(&v.derv[i], sV[u]);
       }
