@@ -1097,7 +1097,7 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
     const int a1 = v.inst_begin[w.x + 1];
     const double w2 = 2.0 * v.inst_df[w.x];
     AgbI<R> I;
-    double se[2], sgx[2], sgy[2], sgz[2], sat[2];
+    AgbP<R> P; /* i-side sums over the run, in R */
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       int i = w.y + 32 * u + lane;
@@ -1109,7 +1109,7 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
       I.b[u] = ok ? Bv[i] : R(1);
       I.c[u] = ok ? GbExp<R>::scale() * BI[i] : R(0);
       I.ia[u] = ok ? i : INT_MAX; /* no valid partner: i < j never holds */
-      se[u] = sgx[u] = sgy[u] = sgz[u] = sat[u] = 0.0;
+      P.e[u] = P.gx[u] = P.gy[u] = P.gz[u] = P.at[u] = R(0);
     }
     for (int k = 0; k < w.w; k++) {
       const int j0 = w.z + 32 * k;
@@ -1123,9 +1123,6 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
       J.b = vj ? Bv[j] : R(1);
       J.bi = vj ? BI[j] : R(0);
       J.gx = J.gy = J.gz = J.at = R(0);
-      AgbP<R> P;
-#pragma unroll
-      for (int u = 0; u < 2; u++) P.e[u] = P.gx[u] = P.gy[u] = P.gz[u] = P.at[u] = R(0);
       if (w.y + 64 <= a1 && j0 >= w.y + 64 && j0 + 32 <= a1) /* warp-uniform */
         agb_tile<R, true>(I, J, P, lane, j0, a1);
       else
@@ -1136,24 +1133,16 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
         atomicAdd(&v.g_gb[3 * j + 2], w2 * (double)J.gz);
         atomicAdd(&v.dera[j], (double)J.at);
       }
-#pragma unroll
-      for (int u = 0; u < 2; u++) {
-        se[u] += (double)P.e[u];
-        sgx[u] += (double)P.gx[u];
-        sgy[u] += (double)P.gy[u];
-        sgz[u] += (double)P.gz[u];
-        sat[u] += (double)P.at[u];
-      }
     }
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       int i = I.ia[u];
       if (i >= a1) continue;
-      atomicAdd(&v.eatom[N + i], C_TOKCAL * w2 * se[u]);
-      atomicAdd(&v.g_gb[3 * i], w2 * sgx[u]);
-      atomicAdd(&v.g_gb[3 * i + 1], w2 * sgy[u]);
-      atomicAdd(&v.g_gb[3 * i + 2], w2 * sgz[u]);
-      atomicAdd(&v.dera[i], sat[u]);
+      atomicAdd(&v.eatom[N + i], C_TOKCAL * w2 * (double)P.e[u]);
+      atomicAdd(&v.g_gb[3 * i], w2 * (double)P.gx[u]);
+      atomicAdd(&v.g_gb[3 * i + 1], w2 * (double)P.gy[u]);
+      atomicAdd(&v.g_gb[3 * i + 2], w2 * (double)P.gz[u]);
+      atomicAdd(&v.dera[i], (double)P.at[u]);
     }
   }
 }
@@ -1274,7 +1263,7 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
     const int a0 = v.inst_begin[w.x], hh = a0 + v.inst_nheavy[w.x], a1 = v.inst_begin[w.x + 1];
     const double kg = f4p * v.inst_df[w.x];
     GbdI<R> I;
-    double sU[2], sV[2], sfx[2], sfy[2], sfz[2], svx[2], svy[2], svz[2];
+    GbdP<R> P; /* i-side sums over the run, in R */
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       int i = w.y + 32 * u + lane;
@@ -1290,7 +1279,7 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       I.ab[u] = ok ? AB[i] : R(0);
       I.ti[u] = ok ? v.rtype[i] : 0;
       I.ia[u] = ok ? i : INT_MAX; /* no valid partner: i < j never holds */
-      sU[u] = sV[u] = sfx[u] = sfy[u] = sfz[u] = svx[u] = svy[u] = svz[u] = 0.0;
+      P.U[u] = P.V[u] = P.fx[u] = P.fy[u] = P.fz[u] = P.vx[u] = P.vy[u] = P.vz[u] = R(0);
     }
     const bool iheavy = w.y + 64 <= hh; /* both i tiles complete and heavy */
     for (int k = 0; k < w.w; k++) {
@@ -1308,9 +1297,6 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       J.ab = vj ? AB[j] : R(0);
       J.t = vj ? v.rtype[j] : 0;
       J.U = J.V = J.fx = J.fy = J.fz = J.vx = J.vy = J.vz = R(0);
-      GbdP<R> P;
-#pragma unroll
-      for (int u = 0; u < 2; u++) P.U[u] = P.V[u] = P.fx[u] = P.fy[u] = P.fz[u] = P.vx[u] = P.vy[u] = P.vz[u] = R(0);
       /* warp-uniform tile class */
       const bool interior = iheavy && j0 >= w.y + 64;
       if (interior && j0 + 32 <= hh)
@@ -1331,31 +1317,20 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
           atomicAdd(&v.derv[j], (double)J.V);
         }
       }
-#pragma unroll
-      for (int u = 0; u < 2; u++) {
-        sU[u] += (double)P.U[u];
-        sV[u] += (double)P.V[u];
-        sfx[u] += (double)P.fx[u];
-        sfy[u] += (double)P.fy[u];
-        sfz[u] += (double)P.fz[u];
-        svx[u] += (double)P.vx[u];
-        svy[u] += (double)P.vy[u];
-        svz[u] += (double)P.vz[u];
-      }
     }
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       int i = I.ia[u];
       if (i >= a1) continue;
-      atomicAdd(&v.g_gb[3 * i], kg * sfx[u]);
-      atomicAdd(&v.g_gb[3 * i + 1], kg * sfy[u]);
-      atomicAdd(&v.g_gb[3 * i + 2], kg * sfz[u]);
-      atomicAdd(&v.g_vw[3 * i], f4p * svx[u]);
-      atomicAdd(&v.g_vw[3 * i + 1], f4p * svy[u]);
-      atomicAdd(&v.g_vw[3 * i + 2], f4p * svz[u]);
+      atomicAdd(&v.g_gb[3 * i], kg * (double)P.fx[u]);
+      atomicAdd(&v.g_gb[3 * i + 1], kg * (double)P.fy[u]);
+      atomicAdd(&v.g_gb[3 * i + 2], kg * (double)P.fz[u]);
+      atomicAdd(&v.g_vw[3 * i], f4p * (double)P.vx[u]);
+      atomicAdd(&v.g_vw[3 * i + 1], f4p * (double)P.vy[u]);
+      atomicAdd(&v.g_vw[3 * i + 2], f4p * (double)P.vz[u]);
       if (I.hi[u]) {
-        atomicAdd(&v.deru[i], sU[u]);
-        atomicAdd(&v.derv[i], sV[u]);
+        atomicAdd(&v.deru[i], (double)P.U[u]);
+        atomicAdd(&v.derv[i], (double)P.V[u]);
       }
     }
   }
