@@ -132,6 +132,22 @@ __device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float m_rsqrt(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double m_rsqrt(double x) { return rsqrt(x); }
 
+/* the pair passes' special functions: in FP32 the single-instruction PTX
+   approximations (relative error near 2^-22, denormals flushed), in FP64
+   the library functions */
+__device__ __forceinline__ float p_sqrt(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ double p_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float p_rsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ double p_rsqrt(double x) { return rsqrt(x); }
+
 template <typename R>
 __device__ __forceinline__ R px(const View &v, int g);
 template <>
@@ -627,7 +643,11 @@ struct GbExp;
 template <>
 struct GbExp<float> {
   static __device__ __forceinline__ float scale() { return -0.25f * 1.4426950408889634f; }
-  static __device__ __forceinline__ float ex(float a) { return exp2f(a); }
+  static __device__ __forceinline__ float ex(float a) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(a));
+    return y;
+  }
 };
 template <>
 struct GbExp<double> {
@@ -736,9 +756,10 @@ struct alignas(2 * sizeof(R)) PartW {
   int t;
 };
 
+/* blocks of ITILE/2 threads, each thread two atoms of the ITILE-atom item */
 template <typename R>
-__global__ void __launch_bounds__(ITILE) k_descreen_t(View v, const int4 *__restrict__ items, int nitems,
-                                                      int nch) {
+__global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__restrict__ items, int nitems,
+                                                          int nch) {
   AGB_SHARED Part4<R> sp4[ITILE];
   AGB_SHARED PartW<R> spw[ITILE];
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
@@ -747,13 +768,22 @@ __global__ void __launch_bounds__(ITILE) k_descreen_t(View v, const int4 *__rest
   const int nt = v.ntypes;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     int4 w = items[it];
-    int g = w.y + threadIdx.x;
-    bool act = g < w.z;
+    int g[2];
+    bool act[2];
+    R xg[2], yg[2], zg[2];
+    int row[2];
+    double acc[2] = {0.0, 0.0};
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      g[u] = w.y + threadIdx.x + u * (ITILE / 2);
+      act[u] = g[u] < w.z;
+      xg[u] = act[u] ? X[g[u]] : R(0);
+      yg[u] = act[u] ? Y[g[u]] : R(0);
+      zg[u] = act[u] ? Z[g[u]] : R(0);
+      row[u] = act[u] ? v.rtype[g[u]] * nt : 0;
+    }
     int p0 = v.inst_begin[w.x], c0, c1;
     chunk_range(p0, p0 + v.inst_nheavy[w.x], w.w, nch, c0, c1);
-    R xg = act ? X[g] : R(0), yg = act ? Y[g] : R(0), zg = act ? Z[g] : R(0);
-    int row = act ? v.rtype[g] * nt : 0;
-    double acc = 0.0;
     for (int j0 = c0; j0 < c1; j0 += ITILE) {
       int n = min(ITILE, c1 - j0);
       AGB_SYNC();
@@ -770,21 +800,25 @@ __global__ void __launch_bounds__(ITILE) k_descreen_t(View v, const int4 *__rest
         spw[t] = b;
       }
       AGB_SYNC();
-      if (act) {
-        R part = R(0);
+      if (act[0]) {
+        R part[2] = {R(0), R(0)};
         for (int t = 0; t < n; t++) {
           Part4<R> a = sp4[t];
-          R dx = a.x - xg, dy = a.y - yg, dz = a.z - zg;
-          R xh = m_sqrt(dx * dx + dy * dy + dz * dz) * a.rh;
-          if (xh < R(AGB_NA - 1) && j0 + t != g) {
-            PartW<R> b = spw[t];
-            part += b.w * spline<R>(tab, row + b.t, xh);
+          PartW<R> b = spw[t];
+#pragma unroll
+          for (int u = 0; u < 2; u++) {
+            R dx = a.x - xg[u], dy = a.y - yg[u], dz = a.z - zg[u];
+            R xh = p_sqrt(dx * dx + dy * dy + dz * dz) * a.rh;
+            if (xh < R(AGB_NA - 1) && j0 + t != g[u]) part[u] += b.w * spline<R>(tab, row[u] + b.t, xh);
           }
         }
-        acc += (double)part;
+        acc[0] += (double)part[0];
+        acc[1] += (double)part[1];
       }
     }
-    if (act) atomicAdd(&v.acc_beta[g], acc);
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+      if (act[u]) atomicAdd(&v.acc_beta[g[u]], acc[u]);
   }
 }
 
@@ -859,7 +893,7 @@ __global__ void __launch_bounds__(ITILE) k_agb_t(View v, const int4 *__restrict_
           if (!(d2 > R(0))) continue; /* the atom itself and coincident atoms */
           R bb = bg * sb[t];
           R et = GbExp<R>::ex(cg * sbi[t] * d2);
-          R f = m_rsqrt(d2 + bb * et);
+          R f = p_rsqrt(d2 + bb * et);
           R qf3 = sq[t] * f * f * f;
           pe += sq[t] * f;
           R mw = (R(1) - R(0.25) * et) * qf3;
@@ -958,7 +992,7 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
           R dx = sx[t] - xg, dy = sy[t] - yg, dz = sz[t] - zg;
           R d2 = dx * dx + dy * dy + dz * dz;
           if (!(d2 > R(0))) continue;
-          R id = m_rsqrt(d2);
+          R id = p_rsqrt(d2);
           R d = d2 * id;
           R ht = R(0), ut = R(0);
           if (heavy) { /* b descreened by a: table (type b, type a), radius of a */
@@ -1037,12 +1071,16 @@ __device__ __forceinline__ T rot1(T x) {
 }
 
 /* agb: GB pair energy, constant-B gradient, A_i (agbnp3_cpu_simd_kernels.c:
-   66-151, 329-460).  Interior j tiles (all valid, after the i block) skip
-   the per-pair index tests. */
+   66-151, 329-460).  A lane keeps AGB_NI i atoms (I+l, I+32+l, ...), so
+   each rotation step evaluates AGB_NI pairs with one set of shuffles.
+   Interior j tiles (all valid, after the i block) skip the per-pair index
+   tests. */
+#define AGB_NI 4
+
 template <typename R>
 struct AgbI {
-  int ia[2];
-  R x[2], y[2], z[2], q[2], b[2], c[2];
+  int ia[AGB_NI];
+  R x[AGB_NI], y[AGB_NI], z[AGB_NI], q[AGB_NI], b[AGB_NI], c[AGB_NI];
 };
 template <typename R>
 struct AgbJ {
@@ -1051,7 +1089,7 @@ struct AgbJ {
 };
 template <typename R>
 struct AgbP {
-  R e[2], gx[2], gy[2], gz[2], at[2];
+  R e[AGB_NI], gx[AGB_NI], gy[AGB_NI], gz[AGB_NI], at[AGB_NI];
 };
 
 template <typename R, bool FULL>
@@ -1064,21 +1102,20 @@ __device__ __forceinline__ void agb_tile(const AgbI<R> &I, AgbJ<R> &J, AgbP<R> &
     const int jr = j0 + ((lane + r) & 31);
     const bool jok = FULL || jr < a1;
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
+    for (int u = 0; u < AGB_NI; u++) {
       R dx = J.x - I.x[u], dy = J.y - I.y[u], dz = J.z - I.z[u];
       R d2 = dx * dx + dy * dy + dz * dz;
       if (!((FULL || (jok && I.ia[u] < jr)) && d2 > R(0))) continue; /* coincident atoms are skipped */
       R bb = I.b[u] * J.b;
       R et = GbExp<R>::ex(I.c[u] * J.bi * d2);
-      R f = m_rsqrt(d2 + bb * et);
-      R qq = I.q[u] * J.q;
-      R qf3 = qq * f * f * f;
-      P.e[u] += qq * f;
-      R mw = (R(1) - R(0.25) * et) * qf3;
-      R gx = mw * dx, gy = mw * dy, gz = mw * dz;
-      P.gx[u] += gx; P.gy[u] += gy; P.gz[u] += gz;
-      J.gx -= gx; J.gy -= gy; J.gz -= gz;
-      R at = (bb + R(0.25) * d2) * et * qf3;
+      R f = p_rsqrt(d2 + bb * et);
+      R qf = I.q[u] * J.q * f;
+      P.e[u] += qf;
+      R qf3 = qf * (f * f), eq = et * qf3;
+      R mw = qf3 - R(0.25) * eq;
+      P.gx[u] = fma(mw, dx, P.gx[u]); P.gy[u] = fma(mw, dy, P.gy[u]); P.gz[u] = fma(mw, dz, P.gz[u]);
+      J.gx = fma(-mw, dx, J.gx); J.gy = fma(-mw, dy, J.gy); J.gz = fma(-mw, dz, J.gz);
+      R at = eq * (bb + R(0.25) * d2);
       P.at[u] += at;
       J.at += at;
     }
@@ -1099,7 +1136,7 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
     AgbI<R> I;
     AgbP<R> P; /* i-side sums over the run, in R */
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
+    for (int u = 0; u < AGB_NI; u++) {
       int i = w.y + 32 * u + lane;
       bool ok = i < a1;
       I.x[u] = ok ? X[i] : R(0);
@@ -1111,6 +1148,7 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
       I.ia[u] = ok ? i : INT_MAX; /* no valid partner: i < j never holds */
       P.e[u] = P.gx[u] = P.gy[u] = P.gz[u] = P.at[u] = R(0);
     }
+    const int iend = w.y + 32 * AGB_NI;
     for (int k = 0; k < w.w; k++) {
       const int j0 = w.z + 32 * k;
       const int j = j0 + lane;
@@ -1123,7 +1161,7 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
       J.b = vj ? Bv[j] : R(1);
       J.bi = vj ? BI[j] : R(0);
       J.gx = J.gy = J.gz = J.at = R(0);
-      if (w.y + 64 <= a1 && j0 >= w.y + 64 && j0 + 32 <= a1) /* warp-uniform */
+      if (iend <= a1 && j0 >= iend && j0 + 32 <= a1) /* warp-uniform */
         agb_tile<R, true>(I, J, P, lane, j0, a1);
       else
         agb_tile<R, false>(I, J, P, lane, j0, a1);
@@ -1135,7 +1173,7 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
       }
     }
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
+    for (int u = 0; u < AGB_NI; u++) {
       int i = I.ia[u];
       if (i >= a1) continue;
       atomicAdd(&v.eatom[N + i], C_TOKCAL * w2 * (double)P.e[u]);
@@ -1216,7 +1254,7 @@ __device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &
       } else if (!(d2 > R(0))) {
         continue; /* coincident atoms */
       }
-      R id = m_rsqrt(d2);
+      R id = p_rsqrt(d2);
       R d = d2 * id;
       R ht = R(0), ut = R(0), q, dq;
       if (hiu && gbd_q4<R, MODE != GBD_GEN>(tv, J.t * nt + I.ti[u], d, I.rh[u], I.ri[u], kref, hinv, q, dq)) {
@@ -1235,12 +1273,10 @@ __device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &
       }
       ht *= id;
       ut *= id;
-      R fx = ht * dx, fy = ht * dy, fz = ht * dz;
-      R ux = ut * dx, uy = ut * dy, uz = ut * dz;
-      P.fx[u] += fx; P.fy[u] += fy; P.fz[u] += fz;
-      P.vx[u] += ux; P.vy[u] += uy; P.vz[u] += uz;
-      J.fx -= fx; J.fy -= fy; J.fz -= fz;
-      J.vx -= ux; J.vy -= uy; J.vz -= uz;
+      P.fx[u] = fma(ht, dx, P.fx[u]); P.fy[u] = fma(ht, dy, P.fy[u]); P.fz[u] = fma(ht, dz, P.fz[u]);
+      P.vx[u] = fma(ut, dx, P.vx[u]); P.vy[u] = fma(ut, dy, P.vy[u]); P.vz[u] = fma(ut, dz, P.vz[u]);
+      J.fx = fma(-ht, dx, J.fx); J.fy = fma(-ht, dy, J.fy); J.fz = fma(-ht, dz, J.fz);
+      J.vx = fma(-ut, dx, J.vx); J.vy = fma(-ut, dy, J.vy); J.vz = fma(-ut, dz, J.vz);
     }
     J.U = rot1(J.U); J.V = rot1(J.V);
     J.fx = rot1(J.fx); J.fy = rot1(J.fy); J.fz = rot1(J.fz);
@@ -2086,28 +2122,35 @@ static int build_items(agb_dev *s, int nch, int jb) {
         it[q].w = c;
         q++;
       }
-  /* symmetric items: 64-atom i blocks, runs of up to jb 32-atom j tiles
-     from the block's first tile to the end of the instance */
-  int cap = 0;
+  /* symmetric items: i blocks of AGB_NI (agb) or 2 (gbders) 32-atom tiles,
+     runs of up to jb 32-atom j tiles from the block's first tile to the
+     end of the instance */
+  int cap_a = 0, cap_g = 0;
   for (int I = 0; I < NI; I++) {
     int T = (ib[I + 1] - ib[I] + 31) / 32;
-    for (int tb = 0; tb < T; tb += 2) cap += (T - tb + jb - 1) / jb;
+    for (int tb = 0; tb < T; tb += AGB_NI) cap_a += (T - tb + jb - 1) / jb;
+    for (int tb = 0; tb < T; tb += 2) cap_g += (T - tb + jb - 1) / jb;
   }
-  int4 *ia = (int4 *)malloc(sizeof(int4) * (cap + 1)), *ig = (int4 *)malloc(sizeof(int4) * (cap + 1));
+  int4 *ia = (int4 *)malloc(sizeof(int4) * (cap_a + 1)), *ig = (int4 *)malloc(sizeof(int4) * (cap_g + 1));
   int na = 0, ng = 0;
   for (int I = 0; I < NI; I++) {
     int a0 = ib[I], n = ib[I + 1] - a0, T = (n + 31) / 32;
     int hh = a0 + inh[I];
-    for (int tb = 0; tb < T; tb += 2)
-      for (int tj = tb; tj < T; tj += jb) {
-        int4 w;
-        w.x = I;
-        w.y = a0 + 32 * tb;
-        w.z = a0 + 32 * tj;
-        w.w = (T - tj) < jb ? (T - tj) : jb;
-        ia[na++] = w;
-        if (w.y < hh) ig[ng++] = w; /* blocks of hydrogens only have no gbders pairs */
-      }
+    for (int pass = 0; pass < 2; pass++) {
+      int step = pass == 0 ? AGB_NI : 2;
+      for (int tb = 0; tb < T; tb += step)
+        for (int tj = tb; tj < T; tj += jb) {
+          int4 w;
+          w.x = I;
+          w.y = a0 + 32 * tb;
+          w.z = a0 + 32 * tj;
+          w.w = (T - tj) < jb ? (T - tj) : jb;
+          if (pass == 0)
+            ia[na++] = w;
+          else if (w.y < hh) /* blocks of hydrogens only have no gbders pairs */
+            ig[ng++] = w;
+        }
+    }
   }
   if (s->items) cudaFree(s->items);
   if (s->items_agb) cudaFree(s->items_agb);
@@ -2453,7 +2496,7 @@ static void launch_all(agb_dev *s) {
   nl += 2;
   stage_mark(s, 4);
   int pgrid = s->nitems < 148 * 16 ? s->nitems : 148 * 16;
-  AGB_LAUNCH(k_descreen_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  AGB_LAUNCH(k_descreen_t<R>, pgrid, ITILE / 2, st, v, s->items, s->nitems, s->nch);
   AGB_LAUNCH(k_born<R>, nblocks(N), BLK, st, v);
   nl += 2;
   stage_mark(s, 5);
