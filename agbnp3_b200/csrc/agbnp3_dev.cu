@@ -656,17 +656,19 @@ struct GbExp<double> {
 };
 
 /* cubic spline of one Q4 table at xh = a / h in [0, AGB_NA-1)
-   (agbnp3_utils.c:229-252), stored per interval k as the cubic in
-   t = xh - k, f = c0 + t (c1 + t (c2 + t c3)), one 16-byte (float) or
-   32-byte (double) record per lookup.  The spline's second derivatives at
-   the interval ends are y2_k = 2 c2 / h^2 and y2_k+1 = (6 c3 + 2 c2) / h^2,
-   so the record also gives d/da:
-     exact:      (c1 + 2 c2 t + 3 c3 t^2) / h
-     reference:  the exact one minus (3 t^2 - 1) h y2_k+1 / 3
+   (agbnp3_utils.c:229-252), divided by the descreening atom's radius R
+   (the same for every atom of its radius type), stored per interval k as
+   the cubic in t = xh - k, Q4/R = c0 + t (c1 + t (c2 + t c3)), one 16-byte
+   (float) or 32-byte (double) record per lookup.  The spline's second
+   derivatives at the interval ends are y2_k = 2 c2 / h^2 and
+   y2_k+1 = (6 c3 + 2 c2) / h^2 (times 1/R), so the record also gives the
+   derivative in t:
+     exact:      c1 + 2 c2 t + 3 c3 t^2
+     reference:  the exact one minus (3 t^2 - 1) h^2 y2_k+1 / 3
                  (agbnp3_utils.c:247-249 adds the y2_k+1 curvature term
                  where the spline derivative subtracts it)
-   i.e. (c1 + k(2 c3 + 2 c2 / 3) + 2 c2 t + (3 c3 - k(6 c3 + 2 c2)) t^2) / h
-   with k = 1 for the reference's sign, 0 for the exact derivative. */
+   i.e. c1 + 2 c3 + 2 c2 / 3 + 2 c2 t - (3 c3 + 2 c2) t^2, and
+   d(Q4/R)/da = (derivative in t) / h. */
 template <typename R>
 struct Tab;
 template <>
@@ -694,14 +696,14 @@ __device__ __forceinline__ R spline(const typename Tab<R>::T *tv, int slot, R xh
   return c.x + t * (c.y + t * (c.z + t * c.w));
 }
 
-/* value and h * d/da; kref = 1 for the reference's derivative, 0 exact */
-template <typename R>
-__device__ __forceinline__ R spline_d(const typename Tab<R>::T *tv, int slot, R xh, R kref, R &fph) {
+/* value and derivative in t; REF: the reference's derivative, else exact */
+template <typename R, bool REF>
+__device__ __forceinline__ R spline_d(const typename Tab<R>::T *tv, int slot, R xh, R &fph) {
   int k = (int)xh;
   R t = xh - R(k);
   typename Tab<R>::T c = Tab<R>::ld(tv + (size_t)slot * AGB_NA + k);
-  R d0 = c.y + kref * (R(2) * c.w + R(2.0 / 3.0) * c.z);
-  R d2 = R(3) * c.w - kref * (R(6) * c.w + R(2) * c.z);
+  R d0 = REF ? c.y + R(2) * c.w + R(2.0 / 3.0) * c.z : c.y;
+  R d2 = REF ? -(R(3) * c.w + R(2) * c.z) : R(3) * c.w;
   fph = d0 + t * (R(2) * c.z + t * d2);
   return c.x + t * (c.y + t * (c.z + t * c.w));
 }
@@ -725,7 +727,6 @@ __global__ void k_pack_sp(View v) {
   AGB_GRID_STRIDE(g, v.natoms) {
     R sp = (R)v.sp[g];
     pa<R>(v, PA_SP)[g] = sp;
-    pa<R>(v, PA_W)[g] = sp * pa<R>(v, PA_RINV)[g];
   }
 }
 
@@ -763,7 +764,7 @@ __global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__
   AGB_SHARED Part4<R> sp4[ITILE];
   AGB_SHARED PartW<R> spw[ITILE];
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
-  const R *RH = pa<R>(v, PA_RH), *W = pa<R>(v, PA_W);
+  const R *RH = pa<R>(v, PA_RH), *W = pa<R>(v, PA_SP); /* the tables carry 1/R of the descreener */
   const typename Tab<R>::T *tab = Tab<R>::val(v);
   const int nt = v.ntypes;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -953,7 +954,8 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
   const R *RH = pa<R>(v, PA_RH), *RI = pa<R>(v, PA_RINV), *SP = pa<R>(v, PA_SP);
   const R *Q2 = pa<R>(v, PA_Q2AB), *AB = pa<R>(v, PA_ABRW);
   const typename Tab<R>::T *tv = Tab<R>::val(v);
-  const R kref = v.compat ? R(1) : R(0), hinv = R((AGB_NA - 1) / C_AMAX);
+  const bool ref = v.compat != 0;
+  const R hinv = R((AGB_NA - 1) / C_AMAX);
   const int nt = v.ntypes;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     int4 w = items[it];
@@ -999,8 +1001,8 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
             R xh = d * rhg;
             if (xh < R(AGB_NA - 1)) {
               R fp;
-              R f = spline_d<R>(tv, st[t] * nt + tg, xh, kref, fp);
-              R q = f * rig, dq = fp * hinv * rig * rig;
+              R f = ref ? spline_d<R, true>(tv, st[t] * nt + tg, xh, fp) : spline_d<R, false>(tv, st[t] * nt + tg, xh, fp);
+              R q = f, dq = fp * hinv * rig;
               pu += sq2[t] * q;
               pv += sab[t] * q;
               ht += sq2[t] * dq * spg;
@@ -1011,8 +1013,11 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
             R xh = d * srh[t];
             if (xh < R(AGB_NA - 1)) {
               R fp;
-              spline_d<R>(tv, tg * nt + st[t], xh, kref, fp);
-              R dq = fp * hinv * sri[t] * sri[t] * ssp[t];
+              if (ref)
+                spline_d<R, true>(tv, tg * nt + st[t], xh, fp);
+              else
+                spline_d<R, false>(tv, tg * nt + st[t], xh, fp);
+              R dq = fp * hinv * sri[t] * ssp[t];
               ht += q2g * dq;
               ut += abg * dq;
             }
@@ -1197,11 +1202,11 @@ template <typename R>
 struct GbdI { /* a lane's two i atoms */
   int ia[2], ti[2];
   bool hi[2];
-  R x[2], y[2], z[2], rh[2], ri[2], sp[2], q2[2], ab[2];
+  R x[2], y[2], z[2], rh[2], sp[2], q2[2], ab[2];
 };
 template <typename R>
 struct GbdJ { /* the j atom a lane holds in a rotation step, and its sums */
-  R x, y, z, rh, ri, sp, q2, ab;
+  R x, y, z, rh, sp, q2, ab;
   int t;
   R U, V, fx, fy, fz, vx, vy, vz;
 };
@@ -1210,35 +1215,33 @@ struct GbdP { /* i-side sums over one j tile */
   R U[2], V[2], fx[2], fy[2], fz[2], vx[2], vy[2], vz[2];
 };
 
-/* Q4 of the atom of type `td` descreened by an atom of 1/(R h) rhs and
-   1/R ris at distance d, and its derivative factor dQ4/dd * ris^2 scale */
-template <typename R, bool SEL>
-__device__ __forceinline__ bool gbd_q4(const typename Tab<R>::T *tv, int slot, R d, R rhs, R ris, R kref, R hinv,
-                                       R &q, R &dq) {
+/* an atom descreened by one of radius R at distance d, rhs = 1/(h R):
+   q = Q4/R and dq = d(Q4/R)/dd = (derivative in t) * rhs */
+template <typename R, bool SEL, bool REF>
+__device__ __forceinline__ bool gbd_q4(const typename Tab<R>::T *tv, int slot, R d, R rhs, R &q, R &dq) {
   R xh = d * rhs;
   bool in = xh < R(AGB_NA - 1);
   if (SEL) {
     R fp;
-    R f = spline_d<R>(tv, slot, in ? xh : R(0), kref, fp);
-    q = in ? f * ris : R(0);
-    dq = in ? fp * hinv * ris * ris : R(0);
+    R f = spline_d<R, REF>(tv, slot, in ? xh : R(0), fp);
+    q = in ? f : R(0);
+    dq = in ? fp * rhs : R(0);
     return true;
   }
   if (!in) return false;
   R fp;
-  R f = spline_d<R>(tv, slot, xh, kref, fp);
-  q = f * ris;
-  dq = fp * hinv * ris * ris;
+  q = spline_d<R, REF>(tv, slot, xh, fp);
+  dq = fp * rhs;
   return true;
 }
 
-template <typename R, int MODE>
+template <typename R, int MODE, bool REF>
 __device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &P, int lane, int j0, int a1, int hh,
-                                         const typename Tab<R>::T *tv, R kref, R hinv, int nt) {
+                                         const typename Tab<R>::T *tv, int nt) {
   for (int r = 0; r < 32; r++) {
     if (r > 0) {
       J.x = rot1(J.x); J.y = rot1(J.y); J.z = rot1(J.z);
-      J.rh = rot1(J.rh); J.ri = rot1(J.ri); J.sp = rot1(J.sp);
+      J.rh = rot1(J.rh); J.sp = rot1(J.sp);
       J.q2 = rot1(J.q2); J.ab = rot1(J.ab); J.t = rot1(J.t);
     }
     const int jr = j0 + ((lane + r) & 31);
@@ -1257,14 +1260,14 @@ __device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &
       R id = p_rsqrt(d2);
       R d = d2 * id;
       R ht = R(0), ut = R(0), q, dq;
-      if (hiu && gbd_q4<R, MODE != GBD_GEN>(tv, J.t * nt + I.ti[u], d, I.rh[u], I.ri[u], kref, hinv, q, dq)) {
+      if (hiu && gbd_q4<R, MODE != GBD_GEN, REF>(tv, J.t * nt + I.ti[u], d, I.rh[u], q, dq)) {
         /* j descreened by i: table (type j, type i), radius of i */
         P.U[u] += J.q2 * q;
         P.V[u] += J.ab * q;
         ht += J.q2 * dq * I.sp[u];
         ut += J.ab * dq * I.sp[u];
       }
-      if (hj && gbd_q4<R, MODE != GBD_GEN>(tv, I.ti[u] * nt + J.t, d, J.rh, J.ri, kref, hinv, q, dq)) {
+      if (hj && gbd_q4<R, MODE != GBD_GEN, REF>(tv, I.ti[u] * nt + J.t, d, J.rh, q, dq)) {
         /* i descreened by j: table (type i, type j), radius of j */
         J.U += I.q2[u] * q;
         J.V += I.ab[u] * q;
@@ -1284,14 +1287,13 @@ __device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &
   }
 }
 
-template <typename R>
+template <typename R, bool REF>
 __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restrict__ items, int nitems) {
   const int lane = threadIdx.x & 31;
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
-  const R *RH = pa<R>(v, PA_RH), *RI = pa<R>(v, PA_RINV), *SP = pa<R>(v, PA_SP);
+  const R *RH = pa<R>(v, PA_RH), *SP = pa<R>(v, PA_SP);
   const R *Q2 = pa<R>(v, PA_Q2AB), *AB = pa<R>(v, PA_ABRW);
   const typename Tab<R>::T *tv = Tab<R>::val(v);
-  const R kref = v.compat ? R(1) : R(0), hinv = R((AGB_NA - 1) / C_AMAX);
   const int nt = v.ntypes;
   const double f4p = 1.0 / (4.0 * C_PI);
   for (int it = blockIdx.x * 4 + (threadIdx.x >> 5); it < nitems; it += gridDim.x * 4) {
@@ -1309,7 +1311,6 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       I.y[u] = ok ? Y[i] : R(0);
       I.z[u] = ok ? Z[i] : R(0);
       I.rh[u] = ok ? RH[i] : R(0);
-      I.ri[u] = ok ? RI[i] : R(0);
       I.sp[u] = ok ? SP[i] : R(0);
       I.q2[u] = ok ? Q2[i] : R(0);
       I.ab[u] = ok ? AB[i] : R(0);
@@ -1327,7 +1328,6 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       J.y = vj ? Y[j] : R(0);
       J.z = vj ? Z[j] : R(0);
       J.rh = vj ? RH[j] : R(0);
-      J.ri = vj ? RI[j] : R(0);
       J.sp = vj ? SP[j] : R(0);
       J.q2 = vj ? Q2[j] : R(0);
       J.ab = vj ? AB[j] : R(0);
@@ -1336,11 +1336,11 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       /* warp-uniform tile class */
       const bool interior = iheavy && j0 >= w.y + 64;
       if (interior && j0 + 32 <= hh)
-        gbd_tile<R, GBD_HH>(I, J, P, lane, j0, a1, hh, tv, kref, hinv, nt);
+        gbd_tile<R, GBD_HH, REF>(I, J, P, lane, j0, a1, hh, tv, nt);
       else if (interior && j0 >= hh && j0 + 32 <= a1)
-        gbd_tile<R, GBD_HX>(I, J, P, lane, j0, a1, hh, tv, kref, hinv, nt);
+        gbd_tile<R, GBD_HX, REF>(I, J, P, lane, j0, a1, hh, tv, nt);
       else
-        gbd_tile<R, GBD_GEN>(I, J, P, lane, j0, a1, hh, tv, kref, hinv, nt);
+        gbd_tile<R, GBD_GEN, REF>(I, J, P, lane, j0, a1, hh, tv, nt);
       if (vj) {
         atomicAdd(&v.g_gb[3 * j], kg * (double)J.fx);
         atomicAdd(&v.g_gb[3 * j + 1], kg * (double)J.fy);
@@ -2255,21 +2255,36 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
          f(t) = c0 + c1 t + c2 t^2 + c3 t^3,
          c0 = y_k,  c1 = y_k+1 - y_k - h^2 (2 y2_k + y2_k+1) / 6,
          c2 = h^2 y2_k / 2,  c3 = h^2 (y2_k+1 - y2_k) / 6.
-       The last node's record is never read: a lookup stops below node
-       AGB_NA-1. */
-    size_t nrec = (size_t)d->ntypes * d->ntypes * AGB_NA;
+       The coefficients are divided by the radius R of the descreening
+       type (the second index of a table), which every atom of that type
+       shares.  The last node's record is never read: a lookup stops below
+       node AGB_NA-1. */
+    const int nt = d->ntypes;
+    double *rt = (double *)malloc(sizeof(double) * (nt > 0 ? nt : 1));
+    for (int t = 0; t < nt; t++) rt[t] = 0.0;
+    for (int g = 0; g < N; g++) {
+      int t = d->rtype[g];
+      if (rt[t] == 0.0) rt[t] = d->r[g];
+      if (rt[t] != d->r[g]) {
+        free(rt);
+        FAIL("atoms %d of radius type %d have radius %.17g, the type %.17g", g, t, d->r[g], rt[t]);
+      }
+    }
+    size_t nrec = (size_t)nt * nt * AGB_NA;
     double *tv = (double *)calloc(nrec * 4, sizeof(double));
     float *fv = (float *)calloc(nrec * 4, sizeof(float));
     const double h = C_AMAX / (AGB_NA - 1), hh6 = h * h / 6.0;
     for (size_t q = 0; q < nrec; q++) {
       if ((int)(q % AGB_NA) == AGB_NA - 1) continue;
+      const double rs = rt[(q / AGB_NA) % nt];
       const double *a = d->tab + q * 2; /* y_k, y2_k, y_k+1, y2_k+1 */
       double c[4] = {a[0], a[2] - a[0] - hh6 * (2.0 * a[1] + a[3]), 0.5 * h * h * a[1], hh6 * (a[3] - a[1])};
       for (int k = 0; k < 4; k++) {
-        tv[4 * q + k] = c[k];
-        fv[4 * q + k] = (float)c[k];
+        tv[4 * q + k] = rs > 0.0 ? c[k] / rs : 0.0;
+        fv[4 * q + k] = (float)tv[4 * q + k];
       }
     }
+    free(rt);
     UP(tabv_d, (const double4 *)tv, nrec, double4);
     UP(tabv_f, (const float4 *)fv, nrec, float4);
     free(tv);
@@ -2509,8 +2524,10 @@ static void launch_all(agb_dev *s) {
   stage_mark(s, 6);
   if (s->tiled_pairs)
     AGB_LAUNCH(k_gbders_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  else if (s->compat)
+    AGB_LAUNCH((k_gbders_sym<R, true>), sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
   else
-    AGB_LAUNCH(k_gbders_sym<R>, sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
+    AGB_LAUNCH((k_gbders_sym<R, false>), sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
   AGB_LAUNCH(k_gbders_post, nblocks(N), BLK, st, v);
   nl += 2;
   stage_mark(s, 7);

@@ -198,16 +198,20 @@ static void build_table(double b, double *out) {
   }
 }
 
+/* radius types: one per distinct radius (agbnp3_utils.c:808-838 groups
+   equal float radii; distinct double radii are kept apart here, so that a
+   type has one exact radius, while each type's table is built from its
+   float radius as in the reference) */
 static int build_tables(inst_t *I) {
-  float radii[MAX_RTYPES];
+  double radii[MAX_RTYPES];
   int nt = 0;
   I->rtype = (int *)malloc(sizeof(int) * I->natoms);
   if (!I->rtype) return -1;
   for (int i = 0; i < I->natoms; i++) {
-    float ri = (float)I->r[i];
+    double ri = I->r[i];
     int t = -1;
     for (int k = 0; k < nt; k++)
-      if (fabsf(ri - radii[k]) < FLT_MIN) {
+      if (ri == radii[k]) {
         t = k;
         break;
       }
@@ -226,7 +230,8 @@ static int build_tables(inst_t *I) {
   if (!I->tab) return -1;
   for (int a = 0; a < nt; a++)
     for (int b = 0; b < nt; b++)
-      build_table(((double)radii[a] - H_RINC) / (double)radii[b], I->tab + (size_t)(a * nt + b) * AGB_NA * 2);
+      build_table(((double)(float)radii[a] - H_RINC) / (double)(float)radii[b],
+                  I->tab + (size_t)(a * nt + b) * AGB_NA * 2);
   return 0;
 }
 
@@ -385,17 +390,17 @@ static int make_dev(inst_t **L, int n, int precision, int compat, int device, ag
 
   /* radius types shared by all members: map each member's types onto a
      common list (first appearance across members) */
-  float radii[MAX_RTYPES];
+  double radii[MAX_RTYPES];
   int ntot = 0;
   int *tmap = (int *)malloc(sizeof(int) * MAX_RTYPES * n);
   for (int k = 0; k < n; k++) {
     inst_t *I = L[k];
-    float loc[MAX_RTYPES];
-    for (int i = 0; i < I->natoms; i++) loc[I->rtype[i]] = (float)I->r[i];
+    double loc[MAX_RTYPES];
+    for (int i = 0; i < I->natoms; i++) loc[I->rtype[i]] = I->r[i];
     for (int t = 0; t < I->ntypes; t++) {
       int f = -1;
       for (int q = 0; q < ntot; q++)
-        if (fabsf(loc[t] - radii[q]) < FLT_MIN) f = q;
+        if (loc[t] == radii[q]) f = q;
       if (f < 0) {
         if (ntot == MAX_RTYPES) {
           errprint("batch: more than %d distinct atomic radii", MAX_RTYPES);
@@ -411,7 +416,8 @@ static int make_dev(inst_t **L, int n, int precision, int compat, int device, ag
   double *tab = (double *)malloc(sizeof(double) * (size_t)nt * nt * AGB_NA * 2);
   for (int a = 0; a < nt; a++)
     for (int b = 0; b < nt; b++)
-      build_table(((double)radii[a] - H_RINC) / (double)radii[b], tab + (size_t)(a * nt + b) * AGB_NA * 2);
+      build_table(((double)(float)radii[a] - H_RINC) / (double)(float)radii[b],
+                  tab + (size_t)(a * nt + b) * AGB_NA * 2);
 
   int g = 0, w = 0;
   for (int k = 0; k < n; k++) {
