@@ -254,6 +254,28 @@ def test_large_fp64_vs_oracle(engine, natoms, seed):
         b.close()
 
 
+def test_mixed_100k_against_fp64(engine):
+    """The 100,000-atom globule: the chosen mode against the plain FP64 path
+    (which matches the oracle to 1e-9 at the sizes the oracle can run):
+    every energy term within 1e-4 relative, forces within 1e-3 RMS relative,
+    and the same near-list and overlap counts (the index sets use the same
+    float tests in both modes)."""
+    s = A.make_globule(100000, 3)
+    a = A.Instance(s, precision=A.PREC_FP64)
+    b = A.Instance(s, precision=A.PREC_MIXED)
+    try:
+        Ra, Rb = a.ener(), b.ener()
+        for k in ("egb", "evdw", "ecav", "ehb", "mol_volume"):
+            assert abs(Rb[k] - Ra[k]) <= 1e-4 * abs(Ra[k]), k
+        ft = lambda R: R["dgbdr"] + R["dvwdr"] + R["decav"] + R["dehb"]  # noqa: E731
+        assert rms_rel(ft(Rb), ft(Ra)) <= 1e-3
+        sa, sb = a.stats(), b.stats()
+        assert sa["near_pairs"] == sb["near_pairs"] and sa["error"] == sb["error"] == 0
+    finally:
+        a.close()
+        b.close()
+
+
 def test_capacity_regrowth(engine, monkeypatch):
     """Near-list and overlap buffers that start far too small overflow, are
     detected through the device error word, regrown and the evaluation is
