@@ -1059,14 +1059,15 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
 }
 
 /* ------------------------------------------------------------------------ */
-/* symmetric pair passes: each warp owns a 64-atom i block (lane l keeps     */
-/* atoms I+l and I+32+l) and walks a run of 32-atom j tiles of the same      */
-/* instance starting at the block.  The j atoms' operands and their partial  */
-/* sums rotate through the warp with __shfl_sync: in step r lane l holds j   */
-/* atom J+((l+r) mod 32), evaluates its pairs with both i atoms when i < j,  */
-/* and after 32 steps each j atom's sums are back in its lane.  Every        */
-/* unordered pair is evaluated once, two per lane and step.  Partial sums    */
-/* are float per j tile, then double.                                        */
+/* symmetric pair passes: each warp owns an i block of NI 32-atom tiles     */
+/* (lane l keeps atoms I+l, I+32+l, ...) and walks a run of 32-atom j tiles  */
+/* of the same instance starting at the block.  The j atoms' operands and    */
+/* their partial sums rotate through the warp with __shfl_sync: in step r    */
+/* lane l holds j atom J+((l+r) mod 32), evaluates its pairs with its NI i   */
+/* atoms when i < j, and after 32 steps each j atom's sums are back in its   */
+/* lane.  Every unordered pair is evaluated once, NI per lane and step.      */
+/* Partial sums are in the working precision over a j tile (j side) or a    */
+/* j run (i side), then double.                                              */
 /* ------------------------------------------------------------------------ */
 #define FULLMASK 0xffffffffu
 
@@ -1080,7 +1081,14 @@ __device__ __forceinline__ T rot1(T x) {
    each rotation step evaluates AGB_NI pairs with one set of shuffles.
    Interior j tiles (all valid, after the i block) skip the per-pair index
    tests. */
-#define AGB_NI 4
+/* i atoms per lane of the symmetric passes: four in FP32, two in FP64 (whose
+   wider registers would otherwise lower the occupancy) */
+template <typename R>
+struct SymNI {
+  static constexpr int agb = sizeof(R) == 4 ? 4 : 2;
+  static constexpr int gbd = sizeof(R) == 4 ? 4 : 2;
+};
+#define AGB_NI (SymNI<R>::agb)
 
 template <typename R>
 struct AgbI {
@@ -1197,12 +1205,13 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
    hydrogens (only "j descreened by i"); those tiles run a rotation loop
    without per-pair flags, the table-range test done by selects. */
 enum { GBD_GEN = 0, GBD_HH = 1, GBD_HX = 2 };
+#define GBD_NI (SymNI<R>::gbd)
 
 template <typename R>
-struct GbdI { /* a lane's two i atoms */
-  int ia[2], ti[2];
-  bool hi[2];
-  R x[2], y[2], z[2], rh[2], sp[2], q2[2], ab[2];
+struct GbdI { /* a lane's i atoms */
+  int ia[GBD_NI], ti[GBD_NI];
+  bool hi[GBD_NI];
+  R x[GBD_NI], y[GBD_NI], z[GBD_NI], rh[GBD_NI], sp[GBD_NI], q2[GBD_NI], ab[GBD_NI];
 };
 template <typename R>
 struct GbdJ { /* the j atom a lane holds in a rotation step, and its sums */
@@ -1212,7 +1221,7 @@ struct GbdJ { /* the j atom a lane holds in a rotation step, and its sums */
 };
 template <typename R>
 struct GbdP { /* i-side sums over one j tile */
-  R U[2], V[2], fx[2], fy[2], fz[2], vx[2], vy[2], vz[2];
+  R U[GBD_NI], V[GBD_NI], fx[GBD_NI], fy[GBD_NI], fz[GBD_NI], vx[GBD_NI], vy[GBD_NI], vz[GBD_NI];
 };
 
 /* an atom descreened by one of radius R at distance d, rhs = 1/(h R):
@@ -1248,7 +1257,7 @@ __device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &
     const bool jok = MODE != GBD_GEN || jr < a1;
     const bool hj = MODE == GBD_HH || (MODE == GBD_GEN && jr < hh);
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
+    for (int u = 0; u < GBD_NI; u++) {
       const bool hiu = MODE != GBD_GEN || I.hi[u];
       R dx = J.x - I.x[u], dy = J.y - I.y[u], dz = J.z - I.z[u];
       R d2 = dx * dx + dy * dy + dz * dz;
@@ -1303,7 +1312,7 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
     GbdI<R> I;
     GbdP<R> P; /* i-side sums over the run, in R */
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
+    for (int u = 0; u < GBD_NI; u++) {
       int i = w.y + 32 * u + lane;
       bool ok = i < a1;
       I.hi[u] = i < hh;
@@ -1318,7 +1327,7 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       I.ia[u] = ok ? i : INT_MAX; /* no valid partner: i < j never holds */
       P.U[u] = P.V[u] = P.fx[u] = P.fy[u] = P.fz[u] = P.vx[u] = P.vy[u] = P.vz[u] = R(0);
     }
-    const bool iheavy = w.y + 64 <= hh; /* both i tiles complete and heavy */
+    const bool iheavy = w.y + 32 * GBD_NI <= hh; /* every i tile complete and heavy */
     for (int k = 0; k < w.w; k++) {
       const int j0 = w.z + 32 * k;
       const int j = j0 + lane;
@@ -1334,7 +1343,7 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       J.t = vj ? v.rtype[j] : 0;
       J.U = J.V = J.fx = J.fy = J.fz = J.vx = J.vy = J.vz = R(0);
       /* warp-uniform tile class */
-      const bool interior = iheavy && j0 >= w.y + 64;
+      const bool interior = iheavy && j0 >= w.y + 32 * GBD_NI;
       if (interior && j0 + 32 <= hh)
         gbd_tile<R, GBD_HH, REF>(I, J, P, lane, j0, a1, hh, tv, nt);
       else if (interior && j0 >= hh && j0 + 32 <= a1)
@@ -1355,7 +1364,7 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       }
     }
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
+    for (int u = 0; u < GBD_NI; u++) {
       int i = I.ia[u];
       if (i >= a1) continue;
       atomicAdd(&v.g_gb[3 * i], kg * (double)P.fx[u]);
@@ -1998,6 +2007,7 @@ struct agb_dev {
   int n_agb, n_gbd;
   int tiled_pairs; /* use the one-sided tiled pair kernels instead */
   int jb;          /* j tiles per symmetric work item */
+  int items_prec;  /* precision the symmetric items were built for (i block size) */
   int *h_inst_nheavy;
 };
 
@@ -2122,14 +2132,17 @@ static int build_items(agb_dev *s, int nch, int jb) {
         it[q].w = c;
         q++;
       }
-  /* symmetric items: i blocks of AGB_NI (agb) or 2 (gbders) 32-atom tiles,
+  /* symmetric items: i blocks of SymNI<R> 32-atom tiles for the precision,
      runs of up to jb 32-atom j tiles from the block's first tile to the
      end of the instance */
+  const bool f32 = s->precision == AGB_PREC_MIXED;
+  const int ni_a = f32 ? SymNI<float>::agb : SymNI<double>::agb, ni_g = f32 ? SymNI<float>::gbd : SymNI<double>::gbd;
+  s->items_prec = s->precision;
   int cap_a = 0, cap_g = 0;
   for (int I = 0; I < NI; I++) {
     int T = (ib[I + 1] - ib[I] + 31) / 32;
-    for (int tb = 0; tb < T; tb += AGB_NI) cap_a += (T - tb + jb - 1) / jb;
-    for (int tb = 0; tb < T; tb += 2) cap_g += (T - tb + jb - 1) / jb;
+    for (int tb = 0; tb < T; tb += ni_a) cap_a += (T - tb + jb - 1) / jb;
+    for (int tb = 0; tb < T; tb += ni_g) cap_g += (T - tb + jb - 1) / jb;
   }
   int4 *ia = (int4 *)malloc(sizeof(int4) * (cap_a + 1)), *ig = (int4 *)malloc(sizeof(int4) * (cap_g + 1));
   int na = 0, ng = 0;
@@ -2137,7 +2150,7 @@ static int build_items(agb_dev *s, int nch, int jb) {
     int a0 = ib[I], n = ib[I + 1] - a0, T = (n + 31) / 32;
     int hh = a0 + inh[I];
     for (int pass = 0; pass < 2; pass++) {
-      int step = pass == 0 ? AGB_NI : 2;
+      int step = pass == 0 ? ni_a : ni_g;
       for (int tb = 0; tb < T; tb += step)
         for (int tj = tb; tj < T; tj += jb) {
           int4 w;
@@ -2430,6 +2443,7 @@ extern "C" int agb_dev_set_mode(agb_dev *s, int precision, int compat) {
   s->precision = precision;
   s->compat = compat != 0;
   s->v.compat = s->compat;
+  if (s->items_agb && s->items_prec != precision && build_items(s, s->nch, s->jb)) return -1;
   return 0;
 }
 
@@ -2511,7 +2525,8 @@ static void launch_all(agb_dev *s) {
   nl += 2;
   stage_mark(s, 4);
   int pgrid = s->nitems < 148 * 16 ? s->nitems : 148 * 16;
-  AGB_LAUNCH(k_descreen_t<R>, pgrid, ITILE / 2, st, v, s->items, s->nitems, s->nch);
+  int dgrid = s->nitems < 148 * 32 ? s->nitems : 148 * 32; /* 64-thread descreening blocks */
+  AGB_LAUNCH(k_descreen_t<R>, dgrid, ITILE / 2, st, v, s->items, s->nitems, s->nch);
   AGB_LAUNCH(k_born<R>, nblocks(N), BLK, st, v);
   nl += 2;
   stage_mark(s, 5);

@@ -276,6 +276,24 @@ def test_mixed_100k_against_fp64(engine):
         b.close()
 
 
+def test_mode_switch_on_one_instance(engine):
+    """Precision and derivative convention switched back and forth on one
+    instance (the captured graph and the pair-stage work lists are rebuilt
+    for each mode) give the oracle's results every time."""
+    s, _ = load_golden("globule2000_hbmix")
+    q = {c: O.oracle_eval(s, compat=c) for c in (True, False)}
+    inst = A.Instance(s, precision=A.PREC_MIXED)
+    try:
+        for prec, compat in [(A.PREC_MIXED, True), (A.PREC_FP64, True), (A.PREC_FP64, False),
+                             (A.PREC_MIXED, False), (A.PREC_MIXED, True), (A.PREC_FP64, True)]:
+            inst.set_mode(prec, compat)
+            inst.set_coords(s.coords())
+            inst.ener_resident()
+            check_vs_oracle(inst.results(), q[compat], prec, f"switch/{PREC_NAMES[prec]}/{compat}")
+    finally:
+        inst.close()
+
+
 def test_capacity_regrowth(engine, monkeypatch):
     """Near-list and overlap buffers that start far too small overflow, are
     detected through the device error word, regrown and the evaluation is
