@@ -1792,7 +1792,8 @@ __global__ void __launch_bounds__(128) k_ws_free(View v) {
 /* inclusive sum of a[] over the run of consecutive lanes holding this
    lane's key (a key may come back in a later run, which is summed apart);
    returns whether this lane ends its run */
-__device__ __forceinline__ bool seg_scan12(double (&a)[12], int key) {
+template <typename T>
+__device__ __forceinline__ bool seg_scan12(T (&a)[12], int key) {
   const int lane = threadIdx.x & 31;
   int kp = __shfl_up_sync(0xffffffffu, key, 1);
   int kn = __shfl_down_sync(0xffffffffu, key, 1);
@@ -1802,13 +1803,16 @@ __device__ __forceinline__ bool seg_scan12(double (&a)[12], int key) {
     bool take = lane - o >= start;
 #pragma unroll
     for (int c = 0; c < 12; c++) {
-      double t = __shfl_up_sync(0xffffffffu, a[c], o);
+      T t = __shfl_up_sync(0xffffffffu, a[c], o);
       if (take) a[c] += t;
     }
   }
   return lane == 31 || kn != key;
 }
 
+/* per record: the contributions to its parents' gradients in the working
+   precision (a warp run is at most 32 records), added to the double
+   gradients by one atomic per run and component */
 template <typename R, int M>
 __global__ void __launch_bounds__(256) k_tree_ders(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
@@ -1827,8 +1831,8 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
     const bool act = q < n;
     int par[M];
     R gdr[M][3], gdR[M], ga[M], gr[M];
-    double wc[M], wv[M], wb[M];
-    double su = 0, sv = 0, sh = 0;
+    R wc[M], wv[M], wb[M];
+    R su = R(0), sv = R(0), sh = R(0);
     R fp = R(0), h3 = R(0), inva = R(0);
 #pragma unroll
     for (int k = 0; k < M; k++) {
@@ -1836,7 +1840,7 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
       gdr[k][0] = gdr[k][1] = gdr[k][2] = R(0);
       gdR[k] = ga[k] = R(0);
       gr[k] = R(1);
-      wc[k] = wv[k] = wb[k] = 0.0;
+      wc[k] = wv[k] = wb[k] = R(0);
     }
     if (act) {
       R cx = rec_get<R>(v, M, q, F_CX), cy = rec_get<R>(v, M, q, F_CY), cz = rec_get<R>(v, M, q, F_CZ);
@@ -1844,15 +1848,16 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
       fp = rec_get<R>(v, M, q, F_FP);
       inva = R(1) / rec_get<R>(v, M, q, F_A);
       double df = v.inst_df[v.inst_of[par[0]]];
+      double du = 0.0, dv = 0.0, dh = 0.0;
 #pragma unroll
       for (int k = 0; k < M; k++) {
         int a = par[k];
-        su += v.deru[a];
-        sv += v.derv[a];
-        sh += v.derh[a];
-        wc[k] = sgn * v.gammap[a];
-        wv[k] = sgn * v.dervs[a];
-        wb[k] = sgn * v.derus[a];
+        du += v.deru[a];
+        dv += v.derv[a];
+        dh += v.derh[a];
+        wc[k] = (R)(sgn * v.gammap[a]);
+        wv[k] = (R)(sgn * v.dervs[a]);
+        wb[k] = (R)(sgn * v.derus[a]);
         ga[k] = atom_alpha<R>(v, a);
         gr[k] = (R)v.r[a];
         R u1 = ga[k] * gvol;
@@ -1865,21 +1870,21 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
         }
         gdR[k] = (R(3) * inva * u1 + R(0.5) * d2 / u1) / gr[k];
       }
-      su *= -df * f4p * coef;
-      sv *= -f4p * coef;
-      sh *= -coef;
+      su = (R)(du * -df * f4p * coef);
+      sv = (R)(dv * -f4p * coef);
+      sh = (R)(dh * -coef);
       h3 = fpp + fp / gvol;
     }
     const R h4 = R(2) * fp * inva;
 #pragma unroll
     for (int ii = 0; ii < M; ii++) {
       /* gradient on parent ii: gb xyz, vdw xyz, hb xyz, cavity xyz */
-      double acc[12];
+      R acc[12];
       R ud = R(-2) * fp * (R(1) - ga[ii] * inva) / gr[ii] + h3 * gdR[ii];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        double ur = (double)(gdr[ii][c] * fp);
-        double dd = (double)(ud * gdr[ii][c]);
+        R ur = gdr[ii][c] * fp;
+        R dd = ud * gdr[ii][c];
         acc[c] = su * ur + wb[ii] * dd;
         acc[3 + c] = sv * ur + wv[ii] * dd;
         acc[6 + c] = sh * ur;
@@ -1891,7 +1896,7 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
         R u1 = h4 * ga[ii] / gr[jj], u2 = h3 * gdR[jj];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          double ur = (double)(u1 * gdr[jj][c] + u2 * gdr[ii][c]);
+          R ur = u1 * gdr[jj][c] + u2 * gdr[ii][c];
           acc[9 + c] += wc[jj] * ur;
           acc[3 + c] += wv[jj] * ur;
           acc[c] += wb[jj] * ur;
@@ -1907,10 +1912,10 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
       if (act && tail) {
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          atomicAdd(&v.g_gb[3 * key + c], acc[c]);
-          atomicAdd(&v.g_vw[3 * key + c], acc[3 + c]);
-          atomicAdd(&v.g_hb[3 * key + c], acc[6 + c]);
-          atomicAdd(&v.g_cav[3 * key + c], acc[9 + c]);
+          atomicAdd(&v.g_gb[3 * key + c], (double)acc[c]);
+          atomicAdd(&v.g_vw[3 * key + c], (double)acc[3 + c]);
+          atomicAdd(&v.g_hb[3 * key + c], (double)acc[6 + c]);
+          atomicAdd(&v.g_cav[3 * key + c], (double)acc[9 + c]);
         }
       }
     }
