@@ -119,8 +119,9 @@ enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m
        DC_N27 = DC_C0 + 2, DC_W27, DC_WSC };
 #define DC_SIZE (DC_C0 + 8)
 
-/* record fields of a kept overlap */
-enum { F_A = 0, F_P, F_CX, F_CY, F_CZ, F_GVOL, F_GVOLP, F_FP, F_FPP, F_NUM };
+/* record fields of a kept overlap, stored contiguously per record (12
+   slots, three 4-wide vectors) */
+enum { F_A = 0, F_P, F_CX, F_CY, F_CZ, F_GVOL, F_GVOLP, F_FP, F_FPP, F_NUM = 12 };
 
 /* ------------------------------------------------------------------------ */
 /* math helpers                                                             */
@@ -407,23 +408,52 @@ __device__ __forceinline__ Ov<R> atom_pair(const View &v, int i, int j) {
 }
 
 template <typename R>
-__device__ __forceinline__ R rec_get(const View &v, int m, int q, int f) {
-  return ((const R *)v.rec[m])[(size_t)f * v.cap[m] + q];
-}
+struct Vec4;
+template <>
+struct Vec4<float> {
+  static __device__ __forceinline__ void st(float *p, float a, float b, float c, float d) {
+    *(float4 *)p = make_float4(a, b, c, d);
+  }
+  static __device__ __forceinline__ void ld(const float *p, float &a, float &b, float &c, float &d) {
+    float4 t = *(const float4 *)p;
+    a = t.x;
+    b = t.y;
+    c = t.z;
+    d = t.w;
+  }
+};
+template <>
+struct Vec4<double> {
+  static __device__ __forceinline__ void st(double *p, double a, double b, double c, double d) {
+    ((double2 *)p)[0] = make_double2(a, b);
+    ((double2 *)p)[1] = make_double2(c, d);
+  }
+  static __device__ __forceinline__ void ld(const double *p, double &a, double &b, double &c, double &d) {
+    double2 t0 = ((const double2 *)p)[0], t1 = ((const double2 *)p)[1];
+    a = t0.x;
+    b = t0.y;
+    c = t1.x;
+    d = t1.y;
+  }
+};
 
 template <typename R>
 __device__ __forceinline__ void rec_put(const View &v, int m, int q, const Ov<R> &o) {
-  R *b = (R *)v.rec[m];
-  size_t c = v.cap[m];
-  b[F_A * c + q] = o.a;
-  b[F_P * c + q] = o.p;
-  b[F_CX * c + q] = o.cx;
-  b[F_CY * c + q] = o.cy;
-  b[F_CZ * c + q] = o.cz;
-  b[F_GVOL * c + q] = o.gvol;
-  b[F_GVOLP * c + q] = o.gvolp;
-  b[F_FP * c + q] = o.fp;
-  b[F_FPP * c + q] = o.fpp;
+  R *b = (R *)v.rec[m] + (size_t)q * F_NUM;
+  Vec4<R>::st(b, o.a, o.p, o.cx, o.cy);
+  Vec4<R>::st(b + 4, o.cz, o.gvol, o.gvolp, o.fp);
+  Vec4<R>::st(b + 8, o.fpp, R(0), R(0), R(0));
+}
+
+template <typename R>
+__device__ __forceinline__ Ov<R> rec_load(const View &v, int m, int q) {
+  const R *b = (const R *)v.rec[m] + (size_t)q * F_NUM;
+  Ov<R> o;
+  R pad;
+  Vec4<R>::ld(b, o.a, o.p, o.cx, o.cy);
+  Vec4<R>::ld(b + 4, o.cz, o.gvol, o.gvolp, o.fp);
+  Vec4<R>::ld(b + 8, o.fpp, pad, pad, pad);
+  return o;
 }
 
 /* self-volume and surface-area contributions of one kept overlap of order
@@ -525,11 +555,11 @@ __global__ void k_lm_count(View v) {
   const int cm = v.cap[M - 1];
   AGB_GRID_STRIDE(a, n) {
     int ge = v.gend[M - 1][a], cnt = 0;
-    R aa = rec_get<R>(v, M - 1, a, F_A), ap = rec_get<R>(v, M - 1, a, F_P);
-    R ax = rec_get<R>(v, M - 1, a, F_CX), ay = rec_get<R>(v, M - 1, a, F_CY), az = rec_get<R>(v, M - 1, a, F_CZ);
+    const Ov<R> oa = rec_load<R>(v, M - 1, a);
     for (int b = a + 1; b < ge; b++) {
       int j = v.par[M - 1][(size_t)(M - 2) * cm + b];
-      Ov<R> ov = ogauss<R>(aa, ap, ax, ay, az, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j), pz<R>(v, j));
+      Ov<R> ov = ogauss<R>(oa.a, oa.p, oa.cx, oa.cy, oa.cz, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j),
+                           pz<R>(v, j));
       if (kept(ov.gvolp)) cnt++;
     }
     v.lv_cnt[M][a] = cnt;
@@ -558,11 +588,11 @@ __global__ void k_lm_emit(View v) {
       par[k] = v.par[M - 1][(size_t)k * cm + a];
       svol[k] = ssurf[k] = 0.0;
     }
-    R aa = rec_get<R>(v, M - 1, a, F_A), ap = rec_get<R>(v, M - 1, a, F_P);
-    R ax = rec_get<R>(v, M - 1, a, F_CX), ay = rec_get<R>(v, M - 1, a, F_CY), az = rec_get<R>(v, M - 1, a, F_CZ);
+    const Ov<R> oa = rec_load<R>(v, M - 1, a);
     for (int b = a + 1; b < ge; b++) {
       int j = v.par[M - 1][(size_t)(M - 2) * cm + b];
-      Ov<R> ov = ogauss<R>(aa, ap, ax, ay, az, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j), pz<R>(v, j));
+      Ov<R> ov = ogauss<R>(oa.a, oa.p, oa.cx, oa.cy, oa.cz, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j),
+                           pz<R>(v, j));
       if (!kept(ov.gvolp)) continue;
 #pragma unroll
       for (int k = 0; k < M - 1; k++) v.par[M][(size_t)k * cn + q] = par[k];
@@ -1843,10 +1873,10 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
       wc[k] = wv[k] = wb[k] = R(0);
     }
     if (act) {
-      R cx = rec_get<R>(v, M, q, F_CX), cy = rec_get<R>(v, M, q, F_CY), cz = rec_get<R>(v, M, q, F_CZ);
-      R gvol = rec_get<R>(v, M, q, F_GVOL), fpp = rec_get<R>(v, M, q, F_FPP);
-      fp = rec_get<R>(v, M, q, F_FP);
-      inva = R(1) / rec_get<R>(v, M, q, F_A);
+      const Ov<R> o = rec_load<R>(v, M, q);
+      R cx = o.cx, cy = o.cy, cz = o.cz, gvol = o.gvol, fpp = o.fpp;
+      fp = o.fp;
+      inva = R(1) / o.a;
       double df = v.inst_df[v.inst_of[par[0]]];
       double du = 0.0, dv = 0.0, dh = 0.0;
 #pragma unroll
