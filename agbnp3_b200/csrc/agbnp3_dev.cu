@@ -2645,7 +2645,9 @@ static int run_once(agb_dev *s) {
 
 extern "C" int agb_dev_evaluate(agb_dev *s) {
   CK(cudaSetDevice(s->device));
-  for (int attempt = 0; attempt < 6; attempt++) {
+  /* each attempt can reveal the overflow of one more buffer (a level's
+     size is only known once the level below fits) */
+  for (int attempt = 0; attempt < 16; attempt++) {
     if (run_once(s)) return -1;
     int dc[DC_SIZE];
     CK(cudaMemcpyAsync(dc, s->v.dc, sizeof(dc), cudaMemcpyDeviceToHost, s->st));

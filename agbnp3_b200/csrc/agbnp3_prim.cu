@@ -10,25 +10,29 @@
 #define SCAN_ITEMS 4 /* items per thread */
 #define SCAN_TILE (SCAN_BLOCK * SCAN_ITEMS)
 
+/* phases 1 and 3 run a fixed grid that loops over the live tiles, so a
+   buffer sized for the worst case costs nothing beyond its live length */
+
 /* phase 1: tile sums */
 __global__ void k_scan_tiles(const int *__restrict__ in, const int *__restrict__ n, int cap, int *__restrict__ tile_sum) {
   __shared__ int sh[32];
-  int len = min(*n, cap);
-  long long base = (long long)blockIdx.x * SCAN_TILE;
-  if (base >= len) return;
-  int s = 0;
-  for (int k = 0; k < SCAN_ITEMS; k++) {
-    long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
-    if (i < len) s += in[i];
-  }
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if (lane == 0) sh[warp] = s;
-  __syncthreads();
-  if (warp == 0) {
-    s = lane < SCAN_BLOCK / 32 ? sh[lane] : 0;
+  const int len = min(*n, cap);
+  for (long long base = (long long)blockIdx.x * SCAN_TILE; base < len; base += (long long)gridDim.x * SCAN_TILE) {
+    int s = 0;
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+      long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
+      if (i < len) s += in[i];
+    }
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) tile_sum[blockIdx.x] = s;
+    if (lane == 0) sh[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+      s = lane < SCAN_BLOCK / 32 ? sh[lane] : 0;
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) tile_sum[base / SCAN_TILE] = s;
+    }
+    __syncthreads(); /* sh is reused by the next tile */
   }
 }
 
@@ -71,47 +75,49 @@ __global__ void k_scan_tile_sums(int *__restrict__ tile_sum, const int *__restri
 __global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, const int *__restrict__ n, int cap,
                              const int *__restrict__ tile_sum) {
   __shared__ int sh[32];
-  int len = min(*n, cap);
-  long long base = (long long)blockIdx.x * SCAN_TILE;
-  if (base >= len) return;
-  int v[SCAN_ITEMS];
-  int s = 0;
-  for (int k = 0; k < SCAN_ITEMS; k++) {
-    long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
-    v[k] = i < len ? in[i] : 0;
-    s += v[k];
-  }
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int x = s;
-  for (int o = 1; o < 32; o <<= 1) {
-    int t = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += t;
-  }
-  if (lane == 31) sh[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    int w = sh[lane];
-    for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += t;
+  const int len = min(*n, cap);
+  for (long long base = (long long)blockIdx.x * SCAN_TILE; base < len; base += (long long)gridDim.x * SCAN_TILE) {
+    int v[SCAN_ITEMS];
+    int s = 0;
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+      long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
+      v[k] = i < len ? in[i] : 0;
+      s += v[k];
     }
-    sh[lane] = w;
-  }
-  __syncthreads();
-  int run = tile_sum[blockIdx.x] + x - s + (warp > 0 ? sh[warp - 1] : 0);
-  for (int k = 0; k < SCAN_ITEMS; k++) {
-    long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
-    if (i < len) out[i] = run;
-    run += v[k];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = s;
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += t;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int w = sh[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += t;
+      }
+      sh[lane] = w;
+    }
+    __syncthreads();
+    int run = tile_sum[base / SCAN_TILE] + x - s + (warp > 0 ? sh[warp - 1] : 0);
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+      long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
+      if (i < len) out[i] = run;
+      run += v[k];
+    }
+    __syncthreads(); /* sh is reused by the next tile */
   }
 }
 
 void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s) {
   int ntiles = (cap + SCAN_TILE - 1) / SCAN_TILE;
   if (ntiles < 1) ntiles = 1;
-  AGB_LAUNCH(k_scan_tiles, ntiles, SCAN_BLOCK, s, in, n, cap, scratch);
+  int grid = ntiles < 148 * 2 ? ntiles : 148 * 2; /* two 1024-thread blocks per SM */
+  AGB_LAUNCH(k_scan_tiles, grid, SCAN_BLOCK, s, in, n, cap, scratch);
   AGB_LAUNCH(k_scan_tile_sums, 1, SCAN_BLOCK, s, scratch, n, cap, total);
-  AGB_LAUNCH(k_scan_apply, ntiles, SCAN_BLOCK, s, in, out, n, cap, scratch);
+  AGB_LAUNCH(k_scan_apply, grid, SCAN_BLOCK, s, in, out, n, cap, scratch);
 }
 
 #define SEG_BLOCK 256
