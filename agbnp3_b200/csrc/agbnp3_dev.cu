@@ -123,6 +123,15 @@ enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m
    slots, three 4-wide vectors) */
 enum { F_A = 0, F_P, F_CX, F_CY, F_CZ, F_GVOL, F_GVOLP, F_FP, F_FPP, F_NUM = 12 };
 
+/* packed per-atom operands, in the working precision: position, 1/R,
+   1/(h R), Gaussian exponent KFC/R^2, sp, charge, B, 1/B, q2ab, abrw */
+enum { PA_X = 0, PA_Y, PA_Z, PA_RINV, PA_RH, PA_SP, PA_ALPHA, PA_Q, PA_B, PA_BINV, PA_Q2AB, PA_ABRW, PA_NUM };
+
+template <typename R>
+__device__ __forceinline__ R *pa(const View &v, int k) {
+  return (R *)v.pa[k];
+}
+
 /* ------------------------------------------------------------------------ */
 /* math helpers                                                             */
 /* ------------------------------------------------------------------------ */
@@ -148,6 +157,22 @@ __device__ __forceinline__ float p_rsqrt(float x) {
   return y;
 }
 __device__ __forceinline__ double p_rsqrt(double x) { return rsqrt(x); }
+
+/* reciprocal and exponential of the FP32 overlap arithmetic: approximations
+   (rcp.approx, ex2.approx; relative error near 2^-22) in float, the exact
+   operations in double */
+__device__ __forceinline__ float f_rcp(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ double f_rcp(double x) { return 1.0 / x; }
+__device__ __forceinline__ float f_exp(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x * 1.4426950408889634f));
+  return y;
+}
+__device__ __forceinline__ double f_exp(double x) { return exp(x); }
 
 template <typename R>
 __device__ __forceinline__ R px(const View &v, int g);
@@ -202,10 +227,10 @@ __device__ __forceinline__ Ov<R> ogauss(R a1, R p1, R x1, R y1, R z1, R a2, R p2
   R dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
   R d2 = dx * dx + dy * dy + dz * dz;
   o.a = a1 + a2;
-  R inv = R(1) / o.a;
-  o.p = p1 * p2 * m_exp(-a1 * a2 * d2 * inv);
+  R inv = f_rcp(o.a);
+  o.p = p1 * p2 * f_exp(-a1 * a2 * d2 * inv);
   R u = R(C_PI) * inv;
-  o.gvol = o.p * u * m_sqrt(u);
+  o.gvol = o.p * u * p_sqrt(u);
   o.cx = inv * (a1 * x1 + a2 * x2);
   o.cy = inv * (a1 * y1 + a2 * y2);
   o.cz = inv * (a1 * z1 + a2 * z2);
@@ -397,8 +422,11 @@ __global__ void k_nl_rank(View v) {
 /* ------------------------------------------------------------------------ */
 template <typename R>
 __device__ __forceinline__ R atom_alpha(const View &v, int g) {
-  R r = (R)v.r[g];
-  return R(C_KFC) / (r * r);
+  return pa<R>(v, PA_ALPHA)[g];
+}
+template <typename R>
+__device__ __forceinline__ R atom_rinv(const View &v, int g) {
+  return pa<R>(v, PA_RINV)[g];
 }
 
 template <typename R>
@@ -462,12 +490,12 @@ template <typename R, int M>
 __device__ __forceinline__ void vol_terms(const View &v, int k, const Ov<R> &o, double &dvol, double &dsurf) {
   const double coef = ((M & 1) ? 1.0 : -1.0) / M; /* (-1)^(M+1) / M */
   const R sgn = (M & 1) ? R(1) : R(-1);           /* M * coef */
-  R h3 = sgn * o.fp * R(3) / o.a, h4 = R(0.5) * sgn * o.fp;
+  R h3 = sgn * o.fp * R(3) * f_rcp(o.a), h4 = R(0.5) * sgn * o.fp;
   R u1 = atom_alpha<R>(v, k) * o.gvol, u2 = R(-2) * u1;
   R v0 = u2 * (px<R>(v, k) - o.cx), v1 = u2 * (py<R>(v, k) - o.cy), v2 = u2 * (pz<R>(v, k) - o.cz);
   R d2 = v0 * v0 + v1 * v1 + v2 * v2;
   dvol = coef * (double)o.gvolp;
-  dsurf = (double)((h3 * u1 + h4 * d2 / u1) / (R)v.r[k]);
+  dsurf = (double)((h3 * u1 + h4 * d2 * f_rcp(u1)) * atom_rinv<R>(v, k));
 }
 
 /* order 2: candidates are the near-list pairs, one thread per entry; the
@@ -657,16 +685,6 @@ __global__ void k_scaling(View v) {
   }
 }
 
-/* ------------------------------------------------------------------------ */
-/* packed per-atom operands of the pair stages, in the working precision    */
-/* ------------------------------------------------------------------------ */
-enum { PA_X = 0, PA_Y, PA_Z, PA_RINV, PA_RH, PA_SP, PA_W, PA_Q, PA_B, PA_BINV, PA_Q2AB, PA_ABRW, PA_NUM };
-
-template <typename R>
-__device__ __forceinline__ R *pa(const View &v, int k) {
-  return (R *)v.pa[k];
-}
-
 /* exp(-d^2 / (4 Bi Bj)) as exp2 of a pre-scaled argument in float */
 template <typename R>
 struct GbExp;
@@ -747,6 +765,7 @@ __global__ void k_pack_geom(View v) {
     pa<R>(v, PA_Z)[g] = pz<R>(v, (int)g);
     pa<R>(v, PA_RINV)[g] = ri;
     pa<R>(v, PA_RH)[g] = ri * R((AGB_NA - 1) / C_AMAX);
+    pa<R>(v, PA_ALPHA)[g] = R(C_KFC) / ((R)v.r[g] * (R)v.r[g]);
     pa<R>(v, PA_Q)[g] = (R)v.charge[g];
     v.acc_beta[g] = 0.0;
   }
@@ -1876,7 +1895,7 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
       const Ov<R> o = rec_load<R>(v, M, q);
       R cx = o.cx, cy = o.cy, cz = o.cz, gvol = o.gvol, fpp = o.fpp;
       fp = o.fp;
-      inva = R(1) / o.a;
+      inva = f_rcp(o.a);
       double df = v.inst_df[v.inst_of[par[0]]];
       double du = 0.0, dv = 0.0, dh = 0.0;
 #pragma unroll
@@ -1889,7 +1908,7 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
         wv[k] = (R)(sgn * v.dervs[a]);
         wb[k] = (R)(sgn * v.derus[a]);
         ga[k] = atom_alpha<R>(v, a);
-        gr[k] = (R)v.r[a];
+        gr[k] = atom_rinv<R>(v, a); /* 1/R */
         R u1 = ga[k] * gvol;
         R xk[3] = {px<R>(v, a) - cx, py<R>(v, a) - cy, pz<R>(v, a) - cz};
         R d2 = R(0);
@@ -1898,19 +1917,19 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
           gdr[k][c] = R(-2) * u1 * xk[c];
           d2 += gdr[k][c] * gdr[k][c];
         }
-        gdR[k] = (R(3) * inva * u1 + R(0.5) * d2 / u1) / gr[k];
+        gdR[k] = (R(3) * inva * u1 + R(0.5) * d2 * f_rcp(u1)) * gr[k];
       }
       su = (R)(du * -df * f4p * coef);
       sv = (R)(dv * -f4p * coef);
       sh = (R)(dh * -coef);
-      h3 = fpp + fp / gvol;
+      h3 = fpp + fp * f_rcp(gvol);
     }
     const R h4 = R(2) * fp * inva;
 #pragma unroll
     for (int ii = 0; ii < M; ii++) {
       /* gradient on parent ii: gb xyz, vdw xyz, hb xyz, cavity xyz */
       R acc[12];
-      R ud = R(-2) * fp * (R(1) - ga[ii] * inva) / gr[ii] + h3 * gdR[ii];
+      R ud = R(-2) * fp * (R(1) - ga[ii] * inva) * gr[ii] + h3 * gdR[ii];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         R ur = gdr[ii][c] * fp;
@@ -1923,7 +1942,7 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
 #pragma unroll
       for (int jj = 0; jj < M; jj++) {
         if (jj == ii) continue;
-        R u1 = h4 * ga[ii] / gr[jj], u2 = h3 * gdR[jj];
+        R u1 = h4 * ga[ii] * gr[jj], u2 = h3 * gdR[jj];
 #pragma unroll
         for (int c = 0; c < 3; c++) {
           R ur = u1 * gdr[jj][c] + u2 * gdr[ii][c];
