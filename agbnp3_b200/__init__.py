@@ -92,6 +92,8 @@ def lib():
         L.agbnp3_autotune.argtypes = [ctypes.c_int, _ip, ctypes.c_int]
         L.agbnp3_batch_autotune.argtypes = [ctypes.c_int, _ip, ctypes.c_int]
         L.agbnp3_measure_peaks.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
+        L.agbnp3_ener_device.argtypes = [ctypes.c_int] + [_vp] * 12
+        L.agbnp3_batch_ener_device.argtypes = [ctypes.c_int] + [_vp] * 12
         _lib = L
     return _lib
 

@@ -1848,7 +1848,8 @@ __device__ __forceinline__ bool seg_scan12(T (&a)[12], int key) {
   int kn = __shfl_down_sync(0xffffffffu, key, 1);
   unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || kp != key);
   int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane))); /* last head at or before this lane */
-  for (int o = 1; o < 32; o <<= 1) {
+  const int span = __reduce_max_sync(0xffffffffu, lane - start);      /* longest run in the warp, minus 1 */
+  for (int o = 1; o <= span; o <<= 1) {
     bool take = lane - o >= start;
 #pragma unroll
     for (int c = 0; c < 12; c++) {
@@ -2052,6 +2053,7 @@ struct agb_dev {
   int graph_ok;
   int timing;
   cudaEvent_t ev[AGB_NSTAGE + 1];
+  cudaEvent_t xev; /* orders the instance stream against a caller's stream */
   double stage_ms[AGB_NSTAGE];
   long long nlaunch;
   long long last_stats[16];
@@ -2465,6 +2467,7 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   }
   if (tree_alloc(s)) return -1;
   for (int k = 0; k <= AGB_NSTAGE; k++) CK(cudaEventCreate(&s->ev[k]));
+  CK(cudaEventCreateWithFlags(&s->xev, cudaEventDisableTiming));
   *out = s;
   return 0;
 }
@@ -2478,6 +2481,7 @@ extern "C" void agb_dev_destroy(agb_dev *s) {
   for (int k = 0; k < s->nallocs; k++) cudaFree(s->allocs[k]);
   for (int k = 0; k <= AGB_NSTAGE; k++)
     if (s->ev[k]) cudaEventDestroy(s->ev[k]);
+  if (s->xev) cudaEventDestroy(s->xev);
   cudaStreamDestroy(s->st);
   if (s->items) cudaFree(s->items);
   if (s->items_agb) cudaFree(s->items_agb);
@@ -2711,6 +2715,40 @@ extern "C" int agb_dev_download(agb_dev *s, double *energies, double *sp, double
   if (decav) CK(cudaMemcpyAsync(decav, v.o_gc, 3 * n, cudaMemcpyDeviceToHost, s->st));
   if (dehb) CK(cudaMemcpyAsync(dehb, v.o_gh, 3 * n, cudaMemcpyDeviceToHost, s->st));
   CK(cudaStreamSynchronize(s->st));
+  return 0;
+}
+
+/* device-array variants: the instance stream first waits for the work
+   already queued on the caller's stream; after the output copies the
+   caller's stream waits for the instance stream */
+extern "C" int agb_dev_upload_coords_dev(agb_dev *s, const double *x, const double *y, const double *z,
+                                         void *stream) {
+  CK(cudaSetDevice(s->device));
+  CK(cudaEventRecord(s->xev, (cudaStream_t)stream));
+  CK(cudaStreamWaitEvent(s->st, s->xev, 0));
+  size_t b = sizeof(double) * s->natoms;
+  CK(cudaMemcpyAsync((void *)s->v.x_ext, x, b, cudaMemcpyDeviceToDevice, s->st));
+  CK(cudaMemcpyAsync((void *)s->v.y_ext, y, b, cudaMemcpyDeviceToDevice, s->st));
+  CK(cudaMemcpyAsync((void *)s->v.z_ext, z, b, cudaMemcpyDeviceToDevice, s->st));
+  return 0;
+}
+
+extern "C" int agb_dev_download_dev(agb_dev *s, double *energies, double *sp, double *br, double *surf_area,
+                                    double *dgbdr, double *dvwdr, double *decav, double *dehb, void *stream) {
+  CK(cudaSetDevice(s->device));
+  size_t n = sizeof(double) * s->natoms;
+  View &v = s->v;
+  const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+  if (energies) CK(cudaMemcpyAsync(energies, s->o_energy, sizeof(double) * 7 * s->ninst, k, s->st));
+  if (sp) CK(cudaMemcpyAsync(sp, v.o_sp, n, k, s->st));
+  if (br) CK(cudaMemcpyAsync(br, v.o_br, n, k, s->st));
+  if (surf_area) CK(cudaMemcpyAsync(surf_area, v.o_sa, n, k, s->st));
+  if (dgbdr) CK(cudaMemcpyAsync(dgbdr, v.o_gb, 3 * n, k, s->st));
+  if (dvwdr) CK(cudaMemcpyAsync(dvwdr, v.o_gv, 3 * n, k, s->st));
+  if (decav) CK(cudaMemcpyAsync(decav, v.o_gc, 3 * n, k, s->st));
+  if (dehb) CK(cudaMemcpyAsync(dehb, v.o_gh, 3 * n, k, s->st));
+  CK(cudaEventRecord(s->xev, s->st));
+  CK(cudaStreamWaitEvent((cudaStream_t)stream, s->xev, 0));
   return 0;
 }
 

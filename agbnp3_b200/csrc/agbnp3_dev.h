@@ -93,6 +93,13 @@ int agb_dev_evaluate(agb_dev *s);
 int agb_dev_download(agb_dev *s, double *energies, double *sp, double *br, double *surf_area, double *dgbdr,
                      double *dvwdr, double *decav, double *dehb);
 
+/* the same with device arrays (caller order) and the caller's stream: the
+   instance's work is ordered after what `stream` has queued, and `stream`
+   waits for the output copies */
+int agb_dev_upload_coords_dev(agb_dev *s, const double *x, const double *y, const double *z, void *stream);
+int agb_dev_download_dev(agb_dev *s, double *energies, double *sp, double *br, double *surf_area, double *dgbdr,
+                         double *dvwdr, double *decav, double *dehb, void *stream);
+
 void *agb_dev_stream(agb_dev *s);
 int agb_dev_set_timing(agb_dev *s, int enable);
 int agb_dev_stage_times(agb_dev *s, double *ms, int n);

@@ -777,6 +777,40 @@ int agbnp3_get_results(int tag, double *energies, double *sp, double *br, double
   return AGBNP_OK;
 }
 
+/* one evaluation from and into device arrays: coordinates in, outputs out,
+   no host copies; ordered after the work queued on `stream` */
+static int ener_device(agb_dev *dev, const char *who, const double *x, const double *y, const double *z,
+                       double *energies, double *sp, double *br, double *surf_area, double *dgbdr, double *dvwdr,
+                       double *decav, double *dehb, void *stream) {
+  if (!x || !y || !z) {
+    errprint("%s: coordinate arrays must not be NULL.", who);
+    return AGBNP_ERR;
+  }
+  if (agb_dev_upload_coords_dev(dev, x, y, z, stream) != 0) {
+    errprint("%s: %s", who, agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  if (eval_dev(dev, who) != AGBNP_OK) return AGBNP_ERR;
+  if (agb_dev_download_dev(dev, energies, sp, br, surf_area, dgbdr, dvwdr, decav, dehb, stream) != 0) {
+    errprint("%s: %s", who, agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  return AGBNP_OK;
+}
+
+int agbnp3_ener_device(int tag, const double *x, const double *y, const double *z, double *energies, double *sp,
+                       double *br, double *surf_area, double *dgbdr, double *dvwdr, double *decav, double *dehb,
+                       void *stream) {
+  inst_t *I = get_inst(tag, "agbnp3_ener_device()");
+  if (!I) return AGBNP_ERR;
+  if (I->ws_error) {
+    errprint("agbnp3_ener_device(): a trigonal out-of-plane acceptor does not have three bonded atoms.");
+    return AGBNP_ERR;
+  }
+  return ener_device(I->dev, "agbnp3_ener_device()", x, y, z, energies, sp, br, surf_area, dgbdr, dvwdr, decav,
+                     dehb, stream);
+}
+
 void *agbnp3_stream(int tag) {
   inst_t *I = get_inst(tag, "agbnp3_stream()");
   return I ? agb_dev_stream(I->dev) : NULL;
@@ -914,6 +948,15 @@ int agbnp3_batch_get_results(int btag, double *energies, double *sp, double *br,
     return AGBNP_ERR;
   }
   return AGBNP_OK;
+}
+
+int agbnp3_batch_ener_device(int btag, const double *x, const double *y, const double *z, double *energies,
+                             double *sp, double *br, double *surf_area, double *dgbdr, double *dvwdr, double *decav,
+                             double *dehb, void *stream) {
+  batch_t *B = get_batch(btag, "agbnp3_batch_ener_device()");
+  if (!B) return AGBNP_ERR;
+  return ener_device(B->dev, "agbnp3_batch_ener_device()", x, y, z, energies, sp, br, surf_area, dgbdr, dvwdr,
+                     decav, dehb, stream);
 }
 
 int agbnp3_batch_set_mode(int btag, int precision, int compat) {

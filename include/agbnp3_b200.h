@@ -40,6 +40,19 @@ int agbnp3_ener_resident(int tag);
 int agbnp3_get_results(int tag, double *energies, double *sp, double *br, double *surf_area, double (*dgbdr)[3],
                        double (*dvwdr)[3], double (*decav)[3], double (*dehb)[3]);
 
+/* one evaluation from and into DEVICE arrays on the instance's GPU (caller
+   order): x, y, z [natoms]; energies [7] as in agbnp3_get_results; sp, br,
+   surf_area [natoms]; gradients [natoms][3]; any output may be NULL.  The
+   work is ordered after what is queued on `stream` (a cudaStream_t, NULL:
+   the legacy default stream) and `stream` waits for the outputs, so a
+   framework calling it on its current stream needs no host copies or
+   synchronisation.  The host returns once the evaluation has finished on
+   the device.  For callers that keep coordinates on the GPU (MD engines,
+   PyTorch); agbnp3_ener with host arrays remains the drop-in call. */
+int agbnp3_ener_device(int tag, const double *x, const double *y, const double *z, double *energies, double *sp,
+                       double *br, double *surf_area, double *dgbdr, double *dvwdr, double *decav, double *dehb,
+                       void *stream);
+
 /* the CUDA stream (cudaStream_t) on which an instance's work runs */
 void *agbnp3_stream(int tag);
 
@@ -82,6 +95,11 @@ int agbnp3_batch_ener_resident(int btag);
 int agbnp3_batch_get_results(int btag, double *energies, double *sp, double *br, double *surf_area,
                              double (*dgbdr)[3], double (*dvwdr)[3], double (*decav)[3], double (*dehb)[3]);
 int agbnp3_batch_set_mode(int btag, int precision, int compat);
+/* agbnp3_ener_device for a batch: arrays span all members, concatenated
+   in member order; energies [7 * members] */
+int agbnp3_batch_ener_device(int btag, const double *x, const double *y, const double *z, double *energies,
+                             double *sp, double *br, double *surf_area, double *dgbdr, double *dvwdr, double *decav,
+                             double *dehb, void *stream);
 void *agbnp3_batch_stream(int btag);
 int agbnp3_batch_stage_timing(int btag, int enable);
 int agbnp3_batch_stage_times(int btag, double *ms, int n);
