@@ -19,7 +19,7 @@ GLOBULE = os.path.join(HERE, "libagbnp3_globule.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SRC = ["agbnp3_dev.cu", "agbnp3_prim.cu", "agbnp3_static.cu", "agbnp3_peaks.cu"]
+CUDA_SRC = ["agbnp3_dev.cu", "agbnp3_prim.cu", "agbnp3_static.cu", "agbnp3_peaks.cu", "agbnp3_mlp.cu"]
 C_SRC = ["agbnp3_host.c", "nblist.c"]
 
 

@@ -122,6 +122,16 @@ int agbnp3_gb_energy_static(int natoms, const double *x, const double *y, const 
                             const double *born_radii, double dielectric_in, double dielectric_out, double *egb,
                             double *dera, double *dgbdr, void *stream);
 
+/* C = A B^T (+ bias) on the 5th-generation tensor cores (tcgen05, FP32
+   accumulation in tensor memory), the layer of the learned surrogate: device
+   arrays bf16 A [M x K] (leading dimension lda), bf16 B [N x K] (ldb), fp32
+   bias [N] or NULL, fp32 C [M x N] (ldc); K a multiple of 16, N <= 256,
+   lda and ldb multiples of 8.  Runs on `stream` and waits for it.  Returns
+   0, or -1 on bad sizes, a CUDA error or an MMA that did not complete.  No
+   counterpart in the reference. */
+int agbnp3_tc_gemm(const void *A, int lda, const void *B, int ldb, const float *bias, float *C, int ldc, int M, int N,
+                   int K, void *stream);
+
 /* Arithmetic peaks of GPU `device` measured by the library's own
    throughput kernels (about 0.1 s): out[0] FP32 flop/s counting an FMA as
    two, out[1] FP64 flop/s, out[2] ex2 special-function op/s, out[3] the
