@@ -35,6 +35,8 @@
 #include "agbnp3_launch.cuh"
 #include "agbnp3_dev.h"
 
+#include <cuda_bf16.h>
+
 #include <float.h>
 #include <limits.h>
 #include <math.h>
@@ -110,6 +112,12 @@ struct View {
   int *ws_srt;                    /* the same candidates in index order */
   int cap_wsc;
   double *acc_beta; /* descreening sums */
+  /* learned surrogate: 32-atom tiles of each instance (from its first atom)
+     with their bounding boxes, and every atom's class (-1: none) */
+  int ntiles;
+  const int *tile_base, *tile_inst;
+  float4 *tile_box;
+  signed char *sclass;
   /* Q4 tables as per-interval cubics in t = a/h - k, c0..c3 */
   const float4 *tabv_f;
   const double4 *tabv_d;
@@ -2359,6 +2367,27 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     free(tv);
     free(fv);
   }
+  {
+    int *tbase = (int *)malloc(sizeof(int) * (NI + 1)), nt = 0;
+    for (int I = 0; I < NI; I++) {
+      tbase[I] = nt;
+      nt += (d->inst_begin[I + 1] - d->inst_begin[I] + 31) / 32;
+    }
+    tbase[NI] = nt;
+    int *tinst = (int *)malloc(sizeof(int) * (nt > 0 ? nt : 1));
+    for (int I = 0; I < NI; I++)
+      for (int t = tbase[I]; t < tbase[I + 1]; t++) tinst[t] = I;
+    v.ntiles = nt;
+    UP(tile_base, tbase, NI + 1, int);
+    UP(tile_inst, tinst, nt, int);
+    DALLOC(v.tile_box, 2 * (size_t)(nt > 0 ? nt : 1), float4);
+    free(tbase);
+    free(tinst);
+    signed char *cls = (signed char *)malloc(N > 0 ? N : 1);
+    memset(cls, 0xff, N > 0 ? N : 1);
+    UP(sclass, cls, N, signed char);
+    free(cls);
+  }
   UP(ws_begin, d->ws_begin, NI + 1, int);
   if (NW > 0) {
     UP(ws_inst, ws_inst, NW, int);
@@ -2807,7 +2836,7 @@ extern "C" long long agb_dev_debug_fetch(agb_dev *s, int what, void *out, long l
   }
   if (what >= DBG_ATOM && what < DBG_ATOM + 32) {
     double *arrs[] = {v.volumep, v.surf, v.surf_f, v.sp, v.spe, v.psvol, v.gammap, v.bfil, v.bder, v.br, v.brw,
-                      v.dera, v.q2ab, v.abrw, v.deru, v.derv, v.derh, v.derus, v.dervs};
+                      v.dera, v.q2ab, v.abrw, v.deru, v.derv, v.derh, v.derus, v.dervs, v.acc_beta};
     int k = what - DBG_ATOM;
     if (k >= (int)(sizeof(arrs) / sizeof(arrs[0])) || cap < N) return -1;
     cudaMemcpy(out, arrs[k], sizeof(double) * N, cudaMemcpyDeviceToHost);
@@ -2902,3 +2931,150 @@ extern "C" int agb_dev_autotune(agb_dev *s, int reps, const int *params_in, int 
   return 0;
 }
 
+
+/* ------------------------------------------------------------------------ */
+/* learned surrogate: radial neighbour features per atom                    */
+/* ------------------------------------------------------------------------ */
+#define SF_NC 5              /* atom classes (C, N, O, S, H by radius) */
+#define SF_NB 32             /* radial basis functions per class */
+#define SF_NF (SF_NC * SF_NB) /* features per atom */
+#define SF_RC 8.0f           /* cutoff (A) */
+#define SF_W 4               /* basis functions each side of the nearest centre */
+
+/* the class of every atom: the class radius within 1e-3 A of its radius */
+__global__ void k_set_class(View v, int nc, float r0, float r1, float r2, float r3, float r4, int *unmatched) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    const float cr[SF_NC] = {r0, r1, r2, r3, r4};
+    float r = (float)(v.r[g] - C_RINC);
+    int c = -1;
+    for (int k = 0; k < nc && k < SF_NC; k++)
+      if (fabsf(r - cr[k]) < 1e-3f) c = k;
+    v.sclass[g] = (signed char)c;
+    if (c < 0) atomicAdd(unmatched, 1);
+  }
+}
+
+/* bounding box of every 32-atom tile (float positions) */
+__global__ void k_tile_box(View v) {
+  AGB_GRID_STRIDE(t, v.ntiles) {
+    int I = v.tile_inst[t];
+    int a1 = v.inst_begin[I + 1];
+    int g0 = v.inst_begin[I] + 32 * ((int)t - v.tile_base[I]), g1 = min(g0 + 32, a1);
+    float lx = FLT_MAX, ly = FLT_MAX, lz = FLT_MAX, hx = -FLT_MAX, hy = -FLT_MAX, hz = -FLT_MAX;
+    for (int g = g0; g < g1; g++) {
+      f4 p = v.pos[g];
+      lx = fminf(lx, p.x);
+      ly = fminf(ly, p.y);
+      lz = fminf(lz, p.z);
+      hx = fmaxf(hx, p.x);
+      hy = fmaxf(hy, p.y);
+      hz = fmaxf(hz, p.z);
+    }
+    v.tile_box[2 * t] = make_float4(lx, ly, lz, 0.f);
+    v.tile_box[2 * t + 1] = make_float4(hx, hy, hz, 0.f);
+  }
+}
+
+/* one neighbour at distance d < SF_RC into a feature row (class c):
+   Gaussians of width equal to their spacing, centres k * SF_RC / (SF_NB-1),
+   times a cosine cutoff; basis functions beyond SF_W spacings of d are not
+   added (they are below e^-8 of the nearest) */
+__device__ __forceinline__ void sf_add(float *row, int c, float d) {
+  const float delta = SF_RC / (SF_NB - 1), inv2s2 = 0.5f / (delta * delta);
+  const float fc = 0.5f * (__cosf(3.14159265358979f * d / SF_RC) + 1.f);
+  const int kc = __float2int_rn(d / delta);
+  const int k0 = max(0, kc - SF_W), k1 = min(SF_NB - 1, kc + SF_W);
+  for (int k = k0; k <= k1; k++) {
+    float u = d - (float)k * delta;
+    row[c * SF_NB + k] += fc * __expf(-u * u * inv2s2);
+  }
+}
+
+/* features of every atom: for each neighbour class, the basis sum over the
+   atoms of that class within SF_RC, plus the atom's own class at d = 0.  One
+   warp per 32-atom tile (lane = atom); neighbour tiles whose boxes are
+   farther than SF_RC are skipped; the j atoms rotate through the warp.  Each
+   lane's row of sums lives in shared memory (stride SF_NF + 1 against bank
+   conflicts).  Output: bf16 [natoms][SF_NF], internal order, each feature
+   (x - mean) * invstd when mean / invstd are given. */
+__global__ void __launch_bounds__(128) k_sfeat(View v, const float *__restrict__ mean,
+                                               const float *__restrict__ invstd, __nv_bfloat16 *__restrict__ out) {
+  extern __shared__ float sacc[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float *row = sacc + (size_t)(w * 32 + lane) * (SF_NF + 1);
+  const float rc2 = SF_RC * SF_RC;
+  for (int t = blockIdx.x * 4 + w; t < v.ntiles; t += gridDim.x * 4) {
+    for (int f = 0; f < SF_NF; f++) row[f] = 0.f;
+    const int I = v.tile_inst[t];
+    const int a0 = v.inst_begin[I], a1 = v.inst_begin[I + 1], tb = v.tile_base[I], te = v.tile_base[I + 1];
+    const int g = a0 + 32 * (t - tb) + lane;
+    const bool vi = g < a1;
+    f4 pi = vi ? v.pos[g] : f4{0.f, 0.f, 0.f, 0.f};
+    const int ci = vi ? v.sclass[g] : -1;
+    if (ci >= 0) sf_add(row, ci, 0.f);
+    const float4 ilo = v.tile_box[2 * t], ihi = v.tile_box[2 * t + 1];
+    for (int jt = tb; jt < te; jt++) {
+      const float4 jlo = v.tile_box[2 * jt], jhi = v.tile_box[2 * jt + 1];
+      float gx = fmaxf(0.f, fmaxf(ilo.x - jhi.x, jlo.x - ihi.x));
+      float gy = fmaxf(0.f, fmaxf(ilo.y - jhi.y, jlo.y - ihi.y));
+      float gz = fmaxf(0.f, fmaxf(ilo.z - jhi.z, jlo.z - ihi.z));
+      if (gx * gx + gy * gy + gz * gz >= rc2) continue; /* warp-uniform */
+      const int j0 = a0 + 32 * (jt - tb);
+      const int j = j0 + lane;
+      f4 pj = j < a1 ? v.pos[j] : f4{0.f, 0.f, 0.f, 0.f};
+      int cj = j < a1 ? v.sclass[j] : -1;
+      for (int r = 0; r < 32; r++) {
+        if (r > 0) {
+          pj.x = __shfl_sync(0xffffffffu, pj.x, (lane + 1) & 31);
+          pj.y = __shfl_sync(0xffffffffu, pj.y, (lane + 1) & 31);
+          pj.z = __shfl_sync(0xffffffffu, pj.z, (lane + 1) & 31);
+          cj = __shfl_sync(0xffffffffu, cj, (lane + 1) & 31);
+        }
+        const int jr = j0 + ((lane + r) & 31);
+        if (!vi || cj < 0 || jr == g) continue;
+        float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+        float d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < rc2) sf_add(row, cj, sqrtf(d2));
+      }
+    }
+    __syncwarp();
+    if (vi)
+      for (int f = 0; f < SF_NF; f++) {
+        float x = row[f];
+        if (mean) x = (x - mean[f]) * invstd[f];
+        out[(size_t)g * SF_NF + f] = __float2bfloat16(x);
+      }
+    __syncwarp();
+  }
+}
+
+extern "C" int agb_dev_surrogate_classes(agb_dev *s, const double *class_radii, int nc, int *unmatched) {
+  if (nc < 1 || nc > SF_NC) FAIL("surrogate: 1 to %d atom classes, not %d", SF_NC, nc);
+  CK(cudaSetDevice(s->device));
+  float r[SF_NC] = {-1.f, -1.f, -1.f, -1.f, -1.f};
+  for (int k = 0; k < nc; k++) r[k] = (float)class_radii[k];
+  int *cnt;
+  CK(cudaMalloc((void **)&cnt, sizeof(int)));
+  CK(cudaMemsetAsync(cnt, 0, sizeof(int), s->st));
+  k_set_class<<<nblocks(s->natoms), BLK, 0, s->st>>>(s->v, nc, r[0], r[1], r[2], r[3], r[4], cnt);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(unmatched, cnt, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  cudaFree(cnt);
+  return 0;
+}
+
+/* features of the coordinates of the last evaluation (internal order) */
+extern "C" int agb_dev_surrogate_features(agb_dev *s, const float *mean, const float *invstd, void *out) {
+  CK(cudaSetDevice(s->device));
+  const int smem = 4 * 32 * (SF_NF + 1) * (int)sizeof(float);
+  CK(cudaFuncSetAttribute(k_sfeat, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_tile_box<<<nblocks(s->v.ntiles), BLK, 0, s->st>>>(s->v);
+  int grid = (s->v.ntiles + 3) / 4;
+  if (grid > 148 * 2) grid = 148 * 2;
+  if (grid < 1) grid = 1;
+  k_sfeat<<<grid, 128, smem, s->st>>>(s->v, mean, invstd, (__nv_bfloat16 *)out);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s->st));
+  return 0;
+}

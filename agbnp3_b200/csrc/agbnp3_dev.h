@@ -100,6 +100,13 @@ int agb_dev_upload_coords_dev(agb_dev *s, const double *x, const double *y, cons
 int agb_dev_download_dev(agb_dev *s, double *energies, double *sp, double *br, double *surf_area, double *dgbdr,
                          double *dvwdr, double *decav, double *dehb, void *stream);
 
+/* learned surrogate: the class of every atom from its radius (class_radii
+   without the 0.5 A increment; *unmatched = atoms of no class), and the
+   radial features (bf16 [natoms][160], internal order) of the coordinates of
+   the last evaluation, normalised by mean / invstd when given */
+int agb_dev_surrogate_classes(agb_dev *s, const double *class_radii, int nc, int *unmatched);
+int agb_dev_surrogate_features(agb_dev *s, const float *mean, const float *invstd, void *out);
+
 void *agb_dev_stream(agb_dev *s);
 int agb_dev_set_timing(agb_dev *s, int enable);
 int agb_dev_stage_times(agb_dev *s, double *ms, int n);

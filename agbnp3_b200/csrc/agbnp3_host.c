@@ -811,6 +811,32 @@ int agbnp3_ener_device(int tag, const double *x, const double *y, const double *
                      dehb, stream);
 }
 
+int agbnp3_surrogate_classes(int tag, const double *class_radii, int nclass, int *unmatched) {
+  inst_t *I = get_inst(tag, "agbnp3_surrogate_classes()");
+  if (!I) return AGBNP_ERR;
+  int u = 0;
+  if (agb_dev_surrogate_classes(I->dev, class_radii, nclass, &u) != 0) {
+    errprint("agbnp3_surrogate_classes(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  if (unmatched) *unmatched = u;
+  return AGBNP_OK;
+}
+
+int agbnp3_surrogate_features(int tag, const float *mean, const float *invstd, void *out) {
+  inst_t *I = get_inst(tag, "agbnp3_surrogate_features()");
+  if (!I) return AGBNP_ERR;
+  if (!out) {
+    errprint("agbnp3_surrogate_features(): NULL output.");
+    return AGBNP_ERR;
+  }
+  if (agb_dev_surrogate_features(I->dev, mean, invstd, out) != 0) {
+    errprint("agbnp3_surrogate_features(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  return AGBNP_OK;
+}
+
 void *agbnp3_stream(int tag) {
   inst_t *I = get_inst(tag, "agbnp3_stream()");
   return I ? agb_dev_stream(I->dev) : NULL;

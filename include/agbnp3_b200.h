@@ -122,6 +122,19 @@ int agbnp3_gb_energy_static(int natoms, const double *x, const double *y, const 
                             const double *born_radii, double dielectric_in, double dielectric_out, double *egb,
                             double *dera, double *dgbdr, void *stream);
 
+/* Learned surrogate inputs.  agbnp3_surrogate_classes assigns each atom
+   the class whose radius (without the 0.5 A increment) is within 1e-3 A of
+   its own (class_radii[nclass], nclass <= 5; *unmatched receives the number
+   of atoms with no class).  agbnp3_surrogate_features writes, for the
+   coordinates of the last evaluation, 160 radial features per atom (per
+   neighbour class, 32 Gaussians of width 8/31 A centred at k * 8/31 A times
+   a cosine cutoff at 8 A, plus the atom's own class at distance 0) as bf16
+   [natoms][160] in the engine's internal order (heavy atoms first) into the
+   device array `out`, each feature (x - mean) * invstd when both are given
+   (device arrays [160]).  No counterpart in the reference. */
+int agbnp3_surrogate_classes(int tag, const double *class_radii, int nclass, int *unmatched);
+int agbnp3_surrogate_features(int tag, const float *mean, const float *invstd, void *out);
+
 /* C = A B^T (+ bias) on the 5th-generation tensor cores (tcgen05, FP32
    accumulation in tensor memory), the layer of the learned surrogate: device
    arrays bf16 A [M x K] (leading dimension lda), bf16 B [N x K] (ldb), fp32

@@ -31,3 +31,40 @@ def test_tc_gemm_matches_torch(M, N, K, lda):
     assert _lib().agbnp3_tc_gemm(_p(Abuf), lda, _p(B), K, _p(b), _p(C), N, M, N, K, None) == 0
     ref = Abuf[:, :K].float() @ B.float().T + b
     assert torch.allclose(C, ref, rtol=1e-4, atol=1e-3 * (K / 128) ** 0.5), (C - ref).abs().max().item()
+
+
+CLASS_RADII = (1.7, 1.55, 1.52, 1.8, 1.15)  # C, N, O, S, H of the globule generator
+
+
+def _features(inst, natoms):
+    L = A.lib()
+    L.agbnp3_surrogate_classes.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    L.agbnp3_surrogate_features.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    cr = (ctypes.c_double * 5)(*CLASS_RADII)
+    un = ctypes.c_int(-1)
+    assert L.agbnp3_surrogate_classes(inst.tag, cr, 5, ctypes.byref(un)) == A.AGBNP_OK
+    out = torch.empty(natoms, 160, dtype=torch.bfloat16, device="cuda")
+    assert L.agbnp3_surrogate_features(inst.tag, None, None, _p(out)) == A.AGBNP_OK
+    return un.value, out.float().cpu().numpy()
+
+
+@pytest.mark.gpu
+def test_features_match_cpu_reference():
+    import numpy as np
+    import surrogate_ref as S
+    from conftest import load_golden
+    s, _ = load_golden("globule300_shuffled")
+    inst = A.Instance(s, precision=A.PREC_MIXED)
+    try:
+        inst.ener()
+        unmatched, F = _features(inst, s.natoms)
+        assert unmatched == 0
+        int2ext, _ = s.internal_order()
+        radii = np.asarray(s.r)[int2ext]
+        cls = np.array([int(np.argmin(np.abs(np.array(CLASS_RADII) - r))) for r in radii])
+        xyz = s.coords()[int2ext].astype(np.float32).astype(np.float64)
+        ref = S.features(xyz, cls)
+        err = np.abs(F - ref)
+        assert (err <= 1e-2 * np.abs(ref) + 2e-3).all(), err.max()
+    finally:
+        inst.close()
