@@ -292,7 +292,7 @@ class Instance:
 
 
 ATOM_ARRAYS = ("volumep", "surf_raw", "surf_area", "sp", "spe", "psvol", "gammap", "br1", "bder", "br", "brw",
-               "dera", "q2ab", "abrw", "deru", "derv", "derh", "derus", "dervs")
+               "dera", "q2ab", "abrw", "deru", "derv", "derh", "derus", "dervs", "desc_sum")
 
 
 class Batch:

@@ -147,3 +147,156 @@ extern "C" int agbnp3_tc_gemm(const void *A, int lda, const void *B, int ldb, co
   if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return -1;
   return tc_last_error() == 0 ? 0 : -1;
 }
+
+/* ------------------------------------------------------------------------ */
+/* elementwise kernels of the MLP's training and inference                  */
+/* ------------------------------------------------------------------------ */
+__device__ __forceinline__ float silu_f(float z) { return z / (1.f + __expf(-z)); }
+__device__ __forceinline__ float dsilu_f(float z) {
+  float s = 1.f / (1.f + __expf(-z));
+  return s * (1.f + z * (1.f - s));
+}
+
+#define EW_GRID(n) (int)(((n) + 255) / 256 < 148 * 32 ? ((n) + 255) / 256 : 148 * 32)
+#define EW_LOOP(i, n) for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+/* H = SiLU(Z) in bf16, row-major (ldh) and / or transposed (Ht[c][row], ldt) */
+__global__ void k_mlp_act(const float *Z, int rows, int n, int ldz, __nv_bfloat16 *H, int ldh, __nv_bfloat16 *Ht,
+                          int ldt) {
+  EW_LOOP(e, (long long)rows * n) {
+    int r = (int)(e / n), c = (int)(e % n);
+    __nv_bfloat16 h = __float2bfloat16(silu_f(Z[(size_t)r * ldz + c]));
+    if (H) H[(size_t)r * ldh + c] = h;
+    if (Ht) Ht[(size_t)c * ldt + r] = h;
+  }
+}
+
+/* dZ = dH * SiLU'(Z) in bf16 (row-major and transposed); db += column sums */
+__global__ void k_mlp_act_grad(const float *dH, const float *Z, int rows, int n, __nv_bfloat16 *dZ,
+                               __nv_bfloat16 *dZt, int ldt, float *db) {
+  EW_LOOP(e, (long long)rows * n) {
+    int r = (int)(e / n), c = (int)(e % n);
+    float g = dH[e] * dsilu_f(Z[e]);
+    if (dZ) dZ[e] = __float2bfloat16(g);
+    if (dZt) dZt[(size_t)c * ldt + r] = __float2bfloat16(g);
+    if (db) atomicAdd(&db[c], g);
+  }
+}
+
+/* loss += scale * sum (Y - T)^2; dY = 2 scale (Y - T) as bf16 [rows][16]
+   (columns >= nout zero) and transposed [nout][ldt]; db += column sums */
+__global__ void k_mlp_mse_grad(const float *Y, const float *T, int rows, int nout, float scale, __nv_bfloat16 *dY16,
+                               __nv_bfloat16 *dYt, int ldt, float *db, float *loss) {
+  EW_LOOP(e, (long long)rows * 16) {
+    int r = (int)(e / 16), c = (int)(e % 16);
+    float g = 0.f;
+    if (c < nout) {
+      float d = Y[(size_t)r * nout + c] - T[(size_t)r * nout + c];
+      g = 2.f * scale * d;
+      atomicAdd(loss, scale * d * d);
+      if (db) atomicAdd(&db[c], g);
+      if (dYt) dYt[(size_t)c * ldt + r] = __float2bfloat16(g);
+    }
+    if (dY16) dY16[e] = __float2bfloat16(g);
+  }
+}
+
+/* Adam step t (1-based) on fp32 parameters */
+__global__ void k_mlp_adam(float *p, const float *g, float *m, float *v, long long n, float lr, float b1, float b2,
+                           float eps, float c1, float c2) {
+  EW_LOOP(i, n) {
+    float gi = g[i];
+    float mi = b1 * m[i] + (1.f - b1) * gi, vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+  }
+}
+
+/* fp32 W [N x K] -> bf16 W [N x K] and / or bf16 W^T [K x ldt] (columns >= N zero) */
+__global__ void k_mlp_pack(const float *W, int N, int K, __nv_bfloat16 *Wb, __nv_bfloat16 *Wt, int ldt) {
+  EW_LOOP(e, (long long)K * ldt) {
+    int k = (int)(e / ldt), n = (int)(e % ldt);
+    float w = n < N ? W[(size_t)n * K + k] : 0.f;
+    if (Wt) Wt[e] = __float2bfloat16(w);
+    if (Wb && n < N) Wb[(size_t)n * K + k] = __float2bfloat16(w);
+  }
+}
+
+/* rows idx[] of a bf16 sample matrix X [*, nin] and fp32 targets T [*, nout]
+   -> Xb [rows][nin], its transpose Xt [nin][ldt], Tb [rows][nout] */
+__global__ void k_mlp_gather(const __nv_bfloat16 *X, const float *T, const long long *idx, int rows, int nin, int nout,
+                             __nv_bfloat16 *Xb, __nv_bfloat16 *Xt, int ldt, float *Tb) {
+  EW_LOOP(e, (long long)rows * nin) {
+    int r = (int)(e / nin), c = (int)(e % nin);
+    __nv_bfloat16 x = X[(size_t)idx[r] * nin + c];
+    if (Xb) Xb[e] = x;
+    if (Xt) Xt[(size_t)c * ldt + r] = x;
+    if (c < nout) Tb[(size_t)r * nout + c] = T[(size_t)idx[r] * nout + c];
+  }
+}
+
+#define EW_RET return cudaGetLastError() == cudaSuccess ? 0 : -1
+
+extern "C" int agbnp3_mlp_act(const float *Z, int rows, int n, int ldz, void *H, int ldh, void *Ht, int ldt,
+                              void *stream) {
+  k_mlp_act<<<EW_GRID((long long)rows * n), 256, 0, (cudaStream_t)stream>>>(Z, rows, n, ldz, (__nv_bfloat16 *)H, ldh,
+                                                                          (__nv_bfloat16 *)Ht, ldt);
+  EW_RET;
+}
+
+extern "C" int agbnp3_mlp_act_grad(const float *dH, const float *Z, int rows, int n, void *dZ, void *dZt, int ldt,
+                                   float *db, void *stream) {
+  k_mlp_act_grad<<<EW_GRID((long long)rows * n), 256, 0, (cudaStream_t)stream>>>(
+      dH, Z, rows, n, (__nv_bfloat16 *)dZ, (__nv_bfloat16 *)dZt, ldt, db);
+  EW_RET;
+}
+
+extern "C" int agbnp3_mlp_mse_grad(const float *Y, const float *T, int rows, int nout, float scale, void *dY16,
+                                   void *dYt, int ldt, float *db, float *loss, void *stream) {
+  if (nout > 16) return -1;
+  k_mlp_mse_grad<<<EW_GRID((long long)rows * 16), 256, 0, (cudaStream_t)stream>>>(
+      Y, T, rows, nout, scale, (__nv_bfloat16 *)dY16, (__nv_bfloat16 *)dYt, ldt, db, loss);
+  EW_RET;
+}
+
+extern "C" int agbnp3_mlp_adam(float *p, const float *g, float *m, float *v, long long n, float lr, float b1,
+                               float b2, float eps, int t, void *stream) {
+  float c1 = 1.f / (1.f - powf(b1, (float)t)), c2 = 1.f / (1.f - powf(b2, (float)t));
+  k_mlp_adam<<<EW_GRID(n), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, n, lr, b1, b2, eps, c1, c2);
+  EW_RET;
+}
+
+extern "C" int agbnp3_mlp_pack(const float *W, int N, int K, void *Wb, void *Wt, int ldt, void *stream) {
+  if (ldt < N) return -1;
+  k_mlp_pack<<<EW_GRID((long long)K * ldt), 256, 0, (cudaStream_t)stream>>>(W, N, K, (__nv_bfloat16 *)Wb,
+                                                                           (__nv_bfloat16 *)Wt, ldt);
+  EW_RET;
+}
+
+extern "C" int agbnp3_mlp_gather(const void *X, const float *T, const long long *idx, int rows, int nin, int nout,
+                                 void *Xb, void *Xt, int ldt, float *Tb, void *stream) {
+  if (nout > nin) return -1;
+  k_mlp_gather<<<EW_GRID((long long)rows * nin), 256, 0, (cudaStream_t)stream>>>(
+      (const __nv_bfloat16 *)X, T, idx, rows, nin, nout, (__nv_bfloat16 *)Xb, (__nv_bfloat16 *)Xt, ldt, Tb);
+  EW_RET;
+}
+
+/* the GEMM without waiting, for the training loop (errors surface through
+   agbnp3_tc_error) */
+extern "C" int agbnp3_tc_gemm_async(const void *A, int lda, const void *B, int ldb, const float *bias, float *C,
+                                    int ldc, int M, int N, int K, void *stream) {
+  return agb_tc_gemm_launch(A, lda, B, ldb, bias, C, ldc, M, N, K, stream);
+}
+
+/* the tensor-core error word (1: an MMA wait gave up since the last reset),
+   read after synchronising `stream`; reset = 1 clears it */
+extern "C" int agbnp3_tc_error(int reset, void *stream) {
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return -1;
+  int e = tc_last_error();
+  if (reset) {
+    int zero = 0;
+    cudaMemcpyToSymbol(g_tc_err, &zero, sizeof(int));
+  }
+  return e;
+}

@@ -1,0 +1,296 @@
+"""Learned surrogate of the per-atom descreening sums and self volumes.
+
+A per-atom MLP (160 radial-feature inputs, two hidden layers of 128 SiLU
+units, 2 outputs) maps an atom's neighbourhood within 8 A to its
+descreening sum S_i = sum_j sp_j Q4_ij (the sum in 1/B_i = 1/R_i - S_i/4pi)
+and its self volume sp_i V_i.  Weights are used in bf16 with fp32
+accumulation; every matrix product of the forward and backward passes is
+the library's tcgen05 GEMM (agbnp3_tc_gemm) and every other step (SiLU and
+its derivative, the loss gradient, Adam, weight packing, batch gathering)
+one of its kernels (agbnp3_mlp_*).  torch only holds the device buffers.
+
+    python -m agbnp3_b200.surrogate train --out model.npz [--conformations 2000 --natoms 5000]
+    python -m agbnp3_b200.surrogate evaluate --model model.npz --natoms 25000
+
+Training data: perturbed conformations (N(0, 0.3 A) coordinate noise) of
+seeded globules, labelled by the plain FP64 path of the engine.
+"""
+import argparse
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import AGBNP_OK, AGBNPError, Instance, PREC_FP64, lib, make_globule
+
+NIN, NH, NOUT = 160, 128, 2
+CLASS_RADII = (1.7, 1.55, 1.52, 1.8, 1.15)  # C, N, O, S, H (A, without the 0.5 A increment)
+ATOM_DESC_SUM, ATOM_SP = 19, 3  # per-atom debug arrays: descreening sum, sp
+
+
+def _bind():
+    L = lib()
+    vp, i, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    L.agbnp3_tc_gemm_async.argtypes = [vp, i, vp, i, vp, vp, i, i, i, i, vp]
+    L.agbnp3_tc_error.argtypes = [i, vp]
+    L.agbnp3_mlp_act.argtypes = [vp, i, i, i, vp, i, vp, i, vp]
+    L.agbnp3_mlp_act_grad.argtypes = [vp, vp, i, i, vp, vp, i, vp, vp]
+    L.agbnp3_mlp_mse_grad.argtypes = [vp, vp, i, i, f, vp, vp, i, vp, vp, vp]
+    L.agbnp3_mlp_adam.argtypes = [vp, vp, vp, vp, ctypes.c_longlong, f, f, f, f, i, vp]
+    L.agbnp3_mlp_pack.argtypes = [vp, i, i, vp, vp, i, vp]
+    L.agbnp3_mlp_gather.argtypes = [vp, vp, vp, i, i, i, vp, vp, i, vp, vp]
+    L.agbnp3_surrogate_classes.argtypes = [i, vp, i, vp]
+    L.agbnp3_surrogate_features.argtypes = [i, vp, vp, vp]
+    return L
+
+
+def _p(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _ok(rc, what):
+    if rc != 0:
+        raise AGBNPError(f"{what} failed ({rc})")
+
+
+class Mlp:
+    """Parameters (fp32 masters, bf16 copies for the GEMMs), Adam state and
+    work buffers of one network; forward / backward by the library's
+    kernels on torch's current stream."""
+
+    def __init__(self, seed=0, batch=4096, lr=1e-3, device="cuda"):
+        self.L = _bind()
+        g = torch.Generator().manual_seed(seed)
+        dev = torch.device(device)
+
+        def init(n, k):
+            return (torch.randn(n, k, generator=g) * (2.0 / k) ** 0.5).to(dev)
+
+        self.p = {"W1": init(NH, NIN), "b1": torch.zeros(NH, device=dev), "W2": init(NH, NH),
+                  "b2": torch.zeros(NH, device=dev), "W3": init(NOUT, NH) * 0.1, "b3": torch.zeros(NOUT, device=dev)}
+        self.m = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        self.v = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        self.g = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        self.t, self.lr, self.batch, self.dev = 0, lr, batch, dev
+        bf = dict(dtype=torch.bfloat16, device=dev)
+        self.W1b, self.W2b, self.W3b = torch.empty(NH, NIN, **bf), torch.empty(NH, NH, **bf), torch.empty(NOUT, NH, **bf)
+        self.W2t, self.W3t = torch.empty(NH, NH, **bf), torch.empty(NH, 16, **bf)
+        self.pack()
+        self._alloc(batch)
+
+    def _alloc(self, B):
+        f32, bf = dict(dtype=torch.float32, device=self.dev), dict(dtype=torch.bfloat16, device=self.dev)
+        self.B = B
+        self.Xb, self.Xt, self.Tb = torch.empty(B, NIN, **bf), torch.empty(NIN, B, **bf), torch.empty(B, NOUT, **f32)
+        self.Z1, self.Z2, self.Y = torch.empty(B, NH, **f32), torch.empty(B, NH, **f32), torch.empty(B, NOUT, **f32)
+        self.H1, self.H1t = torch.empty(B, NH, **bf), torch.empty(NH, B, **bf)
+        self.H2, self.H2t = torch.empty(B, NH, **bf), torch.empty(NH, B, **bf)
+        self.dY16, self.dYt = torch.empty(B, 16, **bf), torch.empty(NOUT, B, **bf)
+        self.dH = torch.empty(B, NH, **f32)
+        self.dZ, self.dZt = torch.empty(B, NH, **bf), torch.empty(NH, B, **bf)
+        self.loss = torch.zeros(1, **f32)
+
+    def _s(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def pack(self):
+        L, s, p = self.L, self._s(), self.p
+        _ok(L.agbnp3_mlp_pack(_p(p["W1"]), NH, NIN, _p(self.W1b), None, NH, s), "pack W1")
+        _ok(L.agbnp3_mlp_pack(_p(p["W2"]), NH, NH, _p(self.W2b), _p(self.W2t), NH, s), "pack W2")
+        _ok(L.agbnp3_mlp_pack(_p(p["W3"]), NOUT, NH, _p(self.W3b), _p(self.W3t), 16, s), "pack W3")
+
+    def _gemm(self, A, lda, B, ldb, bias, C, ldc, M, N, K):
+        _ok(self.L.agbnp3_tc_gemm_async(_p(A), lda, _p(B), ldb, _p(bias), _p(C), ldc, M, N, K, self._s()), "tc_gemm")
+
+    def forward_batch(self, Xb, n):
+        """Y[:n] for bf16 inputs Xb [n, 160] (n <= B); keeps the activations"""
+        L, s, p = self.L, self._s(), self.p
+        self._gemm(Xb, NIN, self.W1b, NIN, p["b1"], self.Z1, NH, n, NH, NIN)
+        _ok(L.agbnp3_mlp_act(_p(self.Z1), n, NH, NH, _p(self.H1), NH, _p(self.H1t), self.B, s), "act1")
+        self._gemm(self.H1, NH, self.W2b, NH, p["b2"], self.Z2, NH, n, NH, NH)
+        _ok(L.agbnp3_mlp_act(_p(self.Z2), n, NH, NH, _p(self.H2), NH, _p(self.H2t), self.B, s), "act2")
+        self._gemm(self.H2, NH, self.W3b, NH, p["b3"], self.Y, NOUT, n, NOUT, NH)
+        return self.Y[:n]
+
+    def gradients(self, X, T, idx):
+        """loss and parameter gradients (self.g) of the batch X[idx], T[idx]"""
+        L, s, B = self.L, self._s(), len(idx)
+        if B != self.B:
+            self._alloc(B)
+        _ok(L.agbnp3_mlp_gather(_p(X), _p(T), _p(idx), B, NIN, NOUT, _p(self.Xb), _p(self.Xt), B, _p(self.Tb), s),
+            "gather")
+        self.forward_batch(self.Xb, B)
+        for v in self.g.values():
+            v.zero_()
+        self.loss.zero_()
+        g = self.g
+        _ok(L.agbnp3_mlp_mse_grad(_p(self.Y), _p(self.Tb), B, NOUT, 1.0 / B, _p(self.dY16), _p(self.dYt), B,
+                                  _p(g["b3"]), _p(self.loss), s), "mse")
+        self._gemm(self.dYt, B, self.H2t, B, None, g["W3"], NH, NOUT, NH, B)
+        self._gemm(self.dY16, 16, self.W3t, 16, None, self.dH, NH, B, NH, 16)
+        _ok(L.agbnp3_mlp_act_grad(_p(self.dH), _p(self.Z2), B, NH, _p(self.dZ), _p(self.dZt), B, _p(g["b2"]), s),
+            "act_grad2")
+        self._gemm(self.dZt, B, self.H1t, B, None, g["W2"], NH, NH, NH, B)
+        self._gemm(self.dZ, NH, self.W2t, NH, None, self.dH, NH, B, NH, NH)
+        _ok(L.agbnp3_mlp_act_grad(_p(self.dH), _p(self.Z1), B, NH, None, _p(self.dZt), B, _p(g["b1"]), s),
+            "act_grad1")
+        self._gemm(self.dZt, B, self.Xt, B, None, g["W1"], NIN, NH, NIN, B)
+        return self.loss
+
+    def step(self, X, T, idx):
+        loss = self.gradients(X, T, idx)
+        self.t += 1
+        for k in self.p:
+            _ok(self.L.agbnp3_mlp_adam(_p(self.p[k]), _p(self.g[k]), _p(self.m[k]), _p(self.v[k]), self.p[k].numel(),
+                                       self.lr, 0.9, 0.999, 1e-8, self.t, self._s()), "adam")
+        self.pack()
+        return loss
+
+    def predict(self, X):
+        """fp32 outputs for bf16 inputs X [n, 160]"""
+        n = len(X)
+        out = torch.empty(n, NOUT, device=self.dev)
+        for r0 in range(0, n, self.B):
+            r1 = min(n, r0 + self.B)
+            out[r0:r1] = self.forward_batch(X[r0:r1], r1 - r0)
+        return out
+
+    def state(self):
+        return {k: v.detach().cpu().numpy() for k, v in self.p.items()}
+
+    def load(self, st):
+        for k in self.p:
+            self.p[k].copy_(torch.as_tensor(st[k], device=self.dev))
+        self.pack()
+
+
+def classes_and_features(inst, natoms, mean=None, invstd=None):
+    """radial features (bf16 [natoms, 160], internal order) of the coordinates
+    of inst's last evaluation"""
+    L = _bind()
+    cr = (ctypes.c_double * len(CLASS_RADII))(*CLASS_RADII)
+    un = ctypes.c_int(0)
+    if L.agbnp3_surrogate_classes(inst.tag, cr, len(CLASS_RADII), ctypes.byref(un)) != AGBNP_OK:
+        raise AGBNPError("agbnp3_surrogate_classes failed")
+    out = torch.empty(natoms, NIN, dtype=torch.bfloat16, device="cuda")
+    if L.agbnp3_surrogate_features(inst.tag, _p(mean), _p(invstd), _p(out)) != AGBNP_OK:
+        raise AGBNPError("agbnp3_surrogate_features failed")
+    return un.value, out
+
+
+def labels(inst, natoms, system):
+    """FP64 labels of the last evaluation, internal order: descreening sum,
+    self volume sp V (hydrogens: 0)"""
+    S = inst.atom_array(ATOM_DESC_SUM)
+    sp = inst.atom_array(ATOM_SP)
+    int2ext, _ = system.internal_order()
+    r = np.asarray(system.r)[int2ext] + 0.5
+    vol = 4.0 / 3.0 * np.pi * r ** 3
+    heavy = np.zeros(natoms, bool)
+    heavy[:system.nheavy] = True
+    return np.stack([S, np.where(heavy, sp * vol, 0.0)], 1)
+
+
+def make_dataset(conformations, natoms, bases=20, noise=0.3, seed=7, log=print):
+    """features (raw, bf16) and FP64 labels of perturbed conformations"""
+    per = max(1, conformations // bases)
+    X, T = [], []
+    rng = np.random.default_rng(seed)
+    t0 = time.time()
+    for b in range(bases):
+        s = make_globule(natoms, seed * 1000 + b)
+        inst = Instance(s, precision=PREC_FP64)
+        for k in range(per if b < bases - 1 else conformations - per * (bases - 1)):
+            xyz = s.coords() + rng.normal(0.0, noise, size=(s.natoms, 3))
+            inst.ener(xyz)
+            sv = s.with_coords(xyz)
+            un, F = classes_and_features(inst, s.natoms)
+            X.append(F)
+            T.append(torch.as_tensor(labels(inst, s.natoms, sv), dtype=torch.float32, device="cuda"))
+        inst.close()
+        log(f"base {b + 1}/{bases}: {len(X)} conformations, {time.time() - t0:.1f} s")
+    return torch.cat(X), torch.cat(T)
+
+
+def train(X, T, epochs=2, batch=4096, lr=1e-3, seed=0, log=print):
+    """normalises inputs and targets and trains one network; returns the model
+    dictionary (parameters + normalisation)"""
+    Xf = X.float()
+    mean = Xf.mean(0)
+    invstd = 1.0 / Xf.std(0).clamp_min(1e-3)
+    Xn = ((Xf - mean) * invstd).to(torch.bfloat16)
+    del Xf
+    tmean, tstd = T.mean(0), T.std(0).clamp_min(1e-6)
+    Tn = (T - tmean) / tstd
+    net = Mlp(seed=seed, batch=batch, lr=lr)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    n = len(Xn)
+    hist = []
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=g, device="cuda")
+        tot, cnt = torch.zeros(1, device="cuda"), 0
+        for r0 in range(0, n - batch + 1, batch):
+            tot += net.step(Xn, Tn, perm[r0:r0 + batch])
+            cnt += 1
+        hist.append(tot.item() / cnt)
+        log(f"epoch {ep + 1}: loss {hist[-1]:.5f} (normalised targets)")
+    if net.L.agbnp3_tc_error(1, None) != 0:
+        raise AGBNPError("a tensor-core MMA did not complete")
+    model = {k: v for k, v in net.state().items()}
+    model.update(fmean=mean.cpu().numpy(), finvstd=invstd.cpu().numpy(), tmean=tmean.cpu().numpy(),
+                 tstd=tstd.cpu().numpy(), loss=np.array(hist))
+    return model
+
+
+def load_model(model, seed=0, batch=4096):
+    net = Mlp(seed=seed, batch=batch)
+    net.load(model)
+    return net
+
+
+def predict_system(net, model, inst, natoms):
+    """predicted (descreening sum, self volume) per atom, internal order, for
+    the coordinates of inst's last evaluation; and the unmatched-atom count"""
+    mean = torch.as_tensor(model["fmean"], device="cuda")
+    invstd = torch.as_tensor(model["finvstd"], device="cuda")
+    un, F = classes_and_features(inst, natoms, mean, invstd)
+    Y = net.predict(F)
+    Y = Y * torch.as_tensor(model["tstd"], device="cuda") + torch.as_tensor(model["tmean"], device="cuda")
+    return un, Y
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cmd", choices=["train", "evaluate"])
+    ap.add_argument("--out", default="surrogate_model.npz")
+    ap.add_argument("--model", default="surrogate_model.npz")
+    ap.add_argument("--conformations", type=int, default=2000)
+    ap.add_argument("--natoms", type=int, default=5000)
+    ap.add_argument("--epochs", type=int, default=2)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args()
+    from . import initialize
+    initialize()
+    if a.cmd == "train":
+        X, T = make_dataset(a.conformations, a.natoms)
+        model = train(X, T, epochs=a.epochs, seed=a.seed)
+        np.savez(a.out, **model)
+        print(f"saved {a.out}")
+    else:
+        model = dict(np.load(a.model))
+        net = load_model(model)
+        s = make_globule(a.natoms, 1)
+        inst = Instance(s, precision=PREC_FP64)
+        inst.ener()
+        un, Y = predict_system(net, model, inst, s.natoms)
+        ref = labels(inst, s.natoms, s)
+        Y = Y.cpu().numpy()
+        for k, name in enumerate(("descreening sum", "self volume")):
+            e = Y[:, k] - ref[:, k]
+            print(f"{name}: rms error {np.sqrt((e ** 2).mean()):.4g}, rms value {np.sqrt((ref[:, k] ** 2).mean()):.4g}, "
+                  f"mean error {e.mean():.4g}, unmatched atoms {un}")
+
+
+if __name__ == "__main__":
+    main()

@@ -145,6 +145,37 @@ int agbnp3_surrogate_features(int tag, const float *mean, const float *invstd, v
 int agbnp3_tc_gemm(const void *A, int lda, const void *B, int ldb, const float *bias, float *C, int ldc, int M, int N,
                    int K, void *stream);
 
+/* Training and inference steps of the learned surrogate's MLP (device
+   arrays, launched on `stream` without waiting; 0 or -1 on bad arguments or
+   a launch error).  No counterpart in the reference.
+   agbnp3_tc_gemm_async   agbnp3_tc_gemm without waiting; agbnp3_tc_error
+                          synchronises `stream` and returns the tensor-core
+                          error word (1: an MMA did not complete), reset = 1
+                          clears it
+   agbnp3_mlp_act         H = SiLU(Z) in bf16, row-major (ldh) and / or
+                          transposed (Ht[col][row], ldt)
+   agbnp3_mlp_act_grad    dZ = dH * SiLU'(Z) in bf16 (row-major, transposed);
+                          db += column sums
+   agbnp3_mlp_mse_grad    loss += scale sum (Y - T)^2; dY = 2 scale (Y - T)
+                          as bf16 [rows][16] and transposed; db += sums
+   agbnp3_mlp_adam        one Adam step (t >= 1) on fp32 parameters
+   agbnp3_mlp_pack        fp32 W [N][K] -> bf16 W and / or bf16 W^T [K][ldt]
+   agbnp3_mlp_gather      rows idx[] of bf16 samples and fp32 targets, with
+                          the transposed batch */
+int agbnp3_tc_gemm_async(const void *A, int lda, const void *B, int ldb, const float *bias, float *C, int ldc, int M,
+                         int N, int K, void *stream);
+int agbnp3_tc_error(int reset, void *stream);
+int agbnp3_mlp_act(const float *Z, int rows, int n, int ldz, void *H, int ldh, void *Ht, int ldt, void *stream);
+int agbnp3_mlp_act_grad(const float *dH, const float *Z, int rows, int n, void *dZ, void *dZt, int ldt, float *db,
+                        void *stream);
+int agbnp3_mlp_mse_grad(const float *Y, const float *T, int rows, int nout, float scale, void *dY16, void *dYt,
+                        int ldt, float *db, float *loss, void *stream);
+int agbnp3_mlp_adam(float *p, const float *g, float *m, float *v, long long n, float lr, float b1, float b2, float eps,
+                    int t, void *stream);
+int agbnp3_mlp_pack(const float *W, int N, int K, void *Wb, void *Wt, int ldt, void *stream);
+int agbnp3_mlp_gather(const void *X, const float *T, const long long *idx, int rows, int nin, int nout, void *Xb,
+                      void *Xt, int ldt, float *Tb, void *stream);
+
 /* Arithmetic peaks of GPU `device` measured by the library's own
    throughput kernels (about 0.1 s): out[0] FP32 flop/s counting an FMA as
    two, out[1] FP64 flop/s, out[2] ex2 special-function op/s, out[3] the

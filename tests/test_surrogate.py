@@ -68,3 +68,50 @@ def test_features_match_cpu_reference():
         assert (err <= 1e-2 * np.abs(ref) + 2e-3).all(), err.max()
     finally:
         inst.close()
+
+
+@pytest.mark.gpu
+def test_mlp_gradients_match_cpu_reference():
+    """One backward pass of the training kernels (tcgen05 GEMMs, SiLU and
+    loss-gradient kernels) against the float64 NumPy reference on the same
+    bf16-rounded inputs and weights."""
+    import numpy as np
+    import surrogate_ref as S
+    from agbnp3_b200.surrogate import Mlp
+    B = 256
+    net = Mlp(seed=3, batch=B)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    X = torch.randn(B, 160, device="cuda", generator=g).to(torch.bfloat16)
+    T = torch.randn(B, 2, device="cuda", generator=g)
+    idx = torch.arange(B, device="cuda")
+    loss = net.gradients(X, T, idx).item()
+    torch.cuda.synchronize()
+    p = {k: (v.to(torch.bfloat16).double() if k.startswith("W") else v.double()).cpu().numpy()
+         for k, v in net.p.items()}
+    ref_loss, ref = S.mlp_grads(p, X.double().cpu().numpy(), T.double().cpu().numpy())
+    assert abs(loss - ref_loss) <= 2e-2 * abs(ref_loss)
+    for k, r in ref.items():
+        got = net.g[k].double().cpu().numpy()
+        rel = np.linalg.norm(got - r) / np.linalg.norm(r)
+        assert rel <= 3e-2, (k, rel)
+
+
+@pytest.mark.gpu
+def test_surrogate_training_reduces_loss():
+    """A short training run on FP64 labels of perturbed globule conformations
+    lowers the loss and predicts held-out descreening sums better than their
+    mean."""
+    import numpy as np
+    from agbnp3_b200 import surrogate as SG
+    X, T = SG.make_dataset(conformations=12, natoms=1500, bases=3, log=lambda *a: None)
+    ntr = 10 * 1500
+    model = SG.train(X[:ntr], T[:ntr], epochs=6, batch=1024, lr=2e-3, log=lambda *a: None)
+    assert model["loss"][-1] < 0.5 * model["loss"][0]
+    net = SG.load_model(model, batch=1024)
+    Xn = ((X[ntr:].float() - torch.as_tensor(model["fmean"], device="cuda"))
+          * torch.as_tensor(model["finvstd"], device="cuda")).to(torch.bfloat16)
+    Y = net.predict(Xn) * torch.as_tensor(model["tstd"], device="cuda") + torch.as_tensor(model["tmean"],
+                                                                                          device="cuda")
+    t = T[ntr:, 0].cpu().numpy()
+    e = Y[:, 0].cpu().numpy() - t
+    assert np.sqrt((e ** 2).mean()) < 0.5 * t.std()
