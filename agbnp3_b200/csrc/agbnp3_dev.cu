@@ -112,12 +112,15 @@ struct View {
   int *ws_srt;                    /* the same candidates in index order */
   int cap_wsc;
   double *acc_beta; /* descreening sums */
-  /* learned surrogate: 32-atom tiles of each instance (from its first atom)
-     with their bounding boxes, and every atom's class (-1: none) */
-  int ntiles;
-  const int *tile_base, *tile_inst;
-  float4 *tile_box;
+  /* learned surrogate: every atom's class (-1: none) and a hashed grid of
+     SF_RC cells over all atoms of each instance (buckets sf_bbegin[I] ..
+     + sf_bmask[I]; slots hold position + class and atom + cell key) */
   signed char *sclass;
+  int sf_nbuckets;
+  const int *sf_bbegin, *sf_bmask;
+  int *sf_bcount, *sf_bstart, *sf_bcursor, *sf_abucket, *sf_dc;
+  f4 *sf_spos;
+  int2 *sf_sid;
   /* Q4 tables as per-interval cubics in t = a/h - k, c0..c3 */
   const float4 *tabv_f;
   const double4 *tabv_d;
@@ -2072,6 +2075,7 @@ struct agb_dev {
   int tiled_pairs; /* use the one-sided tiled pair kernels instead */
   int jb;          /* j tiles per symmetric work item */
   int items_prec;  /* precision the symmetric items were built for (i block size) */
+  int sfeat_ready; /* the feature kernel's shared-memory limit is set */
   int *h_inst_nheavy;
 };
 
@@ -2153,6 +2157,7 @@ static int tree_alloc(agb_dev *s) {
   }
   s->scan_cap = maxcap > s->cap_nl ? maxcap : s->cap_nl;
   if (s->v.nbuckets > s->scan_cap) s->scan_cap = s->v.nbuckets;
+  if (s->v.sf_nbuckets > s->scan_cap) s->scan_cap = s->v.sf_nbuckets;
   if (27 * s->natoms > s->scan_cap) s->scan_cap = 27 * s->natoms;
   if (27 * s->nws > s->scan_cap) s->scan_cap = 27 * s->nws;
   CK(cudaMalloc((void **)&s->scan_scratch, sizeof(int) * ((size_t)s->scan_cap / 1024 + 64)));
@@ -2368,21 +2373,29 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     free(fv);
   }
   {
-    int *tbase = (int *)malloc(sizeof(int) * (NI + 1)), nt = 0;
+    /* the surrogate's grid over all atoms: >= 2 buckets per atom */
+    int *sbb = (int *)malloc(sizeof(int) * (NI + 1)), *sbm = (int *)malloc(sizeof(int) * NI), snb = 0;
     for (int I = 0; I < NI; I++) {
-      tbase[I] = nt;
-      nt += (d->inst_begin[I + 1] - d->inst_begin[I] + 31) / 32;
+      int want = 2 * (d->inst_begin[I + 1] - d->inst_begin[I]), sz = 64;
+      while (sz < want) sz <<= 1;
+      sbb[I] = snb;
+      sbm[I] = sz - 1;
+      snb += sz;
     }
-    tbase[NI] = nt;
-    int *tinst = (int *)malloc(sizeof(int) * (nt > 0 ? nt : 1));
-    for (int I = 0; I < NI; I++)
-      for (int t = tbase[I]; t < tbase[I + 1]; t++) tinst[t] = I;
-    v.ntiles = nt;
-    UP(tile_base, tbase, NI + 1, int);
-    UP(tile_inst, tinst, nt, int);
-    DALLOC(v.tile_box, 2 * (size_t)(nt > 0 ? nt : 1), float4);
-    free(tbase);
-    free(tinst);
+    sbb[NI] = snb;
+    v.sf_nbuckets = snb;
+    UP(sf_bbegin, sbb, NI + 1, int);
+    UP(sf_bmask, sbm, NI, int);
+    DALLOC(v.sf_bcount, snb, int);
+    DALLOC(v.sf_bstart, snb, int);
+    DALLOC(v.sf_bcursor, snb, int);
+    DALLOC(v.sf_abucket, N > 0 ? N : 1, int);
+    DALLOC(v.sf_spos, N > 0 ? N : 1, f4);
+    DALLOC(v.sf_sid, N > 0 ? N : 1, int2);
+    DALLOC(v.sf_dc, 2, int);
+    if (upload(v.sf_dc, &snb, sizeof(int))) return -1;
+    free(sbb);
+    free(sbm);
     signed char *cls = (signed char *)malloc(N > 0 ? N : 1);
     memset(cls, 0xff, N > 0 ? N : 1);
     UP(sclass, cls, N, signed char);
@@ -2954,24 +2967,33 @@ __global__ void k_set_class(View v, int nc, float r0, float r1, float r2, float 
   }
 }
 
-/* bounding box of every 32-atom tile (float positions) */
-__global__ void k_tile_box(View v) {
-  AGB_GRID_STRIDE(t, v.ntiles) {
-    int I = v.tile_inst[t];
-    int a1 = v.inst_begin[I + 1];
-    int g0 = v.inst_begin[I] + 32 * ((int)t - v.tile_base[I]), g1 = min(g0 + 32, a1);
-    float lx = FLT_MAX, ly = FLT_MAX, lz = FLT_MAX, hx = -FLT_MAX, hy = -FLT_MAX, hz = -FLT_MAX;
-    for (int g = g0; g < g1; g++) {
-      f4 p = v.pos[g];
-      lx = fminf(lx, p.x);
-      ly = fminf(ly, p.y);
-      lz = fminf(lz, p.z);
-      hx = fmaxf(hx, p.x);
-      hy = fmaxf(hy, p.y);
-      hz = fmaxf(hz, p.z);
-    }
-    v.tile_box[2 * t] = make_float4(lx, ly, lz, 0.f);
-    v.tile_box[2 * t + 1] = make_float4(hx, hy, hz, 0.f);
+/* the surrogate's grid: bucket of every atom (cell edge SF_RC) */
+__device__ __forceinline__ int sf_key(int cx, int cy, int cz) {
+  return (cx & 1023) | ((cy & 1023) << 10) | ((cz & 1023) << 20);
+}
+
+__global__ void k_sf_cell_count(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int I = v.inst_of[g];
+    f4 p = v.pos[g];
+    int cx, cy, cz;
+    cell_of(p.x, p.y, p.z, 1.0f / SF_RC, cx, cy, cz);
+    int b = v.sf_bbegin[I] + cell_hash(cx, cy, cz, v.sf_bmask[I]);
+    v.sf_abucket[g] = b;
+    atomicAdd(&v.sf_bcount[b], 1);
+  }
+}
+
+__global__ void k_sf_cell_fill(View v) {
+  AGB_GRID_STRIDE(g, v.natoms) {
+    f4 p = v.pos[g];
+    int cx, cy, cz;
+    cell_of(p.x, p.y, p.z, 1.0f / SF_RC, cx, cy, cz);
+    int b = v.sf_abucket[g];
+    int slot = v.sf_bstart[b] + atomicAdd(&v.sf_bcursor[b], 1);
+    p.w = (float)v.sclass[g];
+    v.sf_spos[slot] = p;
+    v.sf_sid[slot] = make_int2((int)g, sf_key(cx, cy, cz));
   }
 }
 
@@ -2992,59 +3014,46 @@ __device__ __forceinline__ void sf_add(float *row, int c, float d) {
 
 /* features of every atom: for each neighbour class, the basis sum over the
    atoms of that class within SF_RC, plus the atom's own class at d = 0.  One
-   warp per 32-atom tile (lane = atom); neighbour tiles whose boxes are
-   farther than SF_RC are skipped; the j atoms rotate through the warp.  Each
-   lane's row of sums lives in shared memory (stride SF_NF + 1 against bank
-   conflicts).  Output: bf16 [natoms][SF_NF], internal order, each feature
-   (x - mean) * invstd when mean / invstd are given. */
-__global__ void __launch_bounds__(128) k_sfeat(View v, const float *__restrict__ mean,
-                                               const float *__restrict__ invstd, __nv_bfloat16 *__restrict__ out) {
+   thread per atom scans the 27 grid cells around its own; its row of sums
+   lives in shared memory (stride SF_NF + 1).  Output: bf16
+   [natoms][SF_NF], internal order, each feature (x - mean) * invstd when
+   mean / invstd are given. */
+#define SF_BLOCK 64
+__global__ void __launch_bounds__(SF_BLOCK) k_sfeat(View v, const float *__restrict__ mean,
+                                                    const float *__restrict__ invstd, __nv_bfloat16 *__restrict__ out) {
   extern __shared__ float sacc[];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  float *row = sacc + (size_t)(w * 32 + lane) * (SF_NF + 1);
+  float *row = sacc + (size_t)threadIdx.x * (SF_NF + 1);
   const float rc2 = SF_RC * SF_RC;
-  for (int t = blockIdx.x * 4 + w; t < v.ntiles; t += gridDim.x * 4) {
-    for (int f = 0; f < SF_NF; f++) row[f] = 0.f;
-    const int I = v.tile_inst[t];
-    const int a0 = v.inst_begin[I], a1 = v.inst_begin[I + 1], tb = v.tile_base[I], te = v.tile_base[I + 1];
-    const int g = a0 + 32 * (t - tb) + lane;
-    const bool vi = g < a1;
-    f4 pi = vi ? v.pos[g] : f4{0.f, 0.f, 0.f, 0.f};
-    const int ci = vi ? v.sclass[g] : -1;
-    if (ci >= 0) sf_add(row, ci, 0.f);
-    const float4 ilo = v.tile_box[2 * t], ihi = v.tile_box[2 * t + 1];
-    for (int jt = tb; jt < te; jt++) {
-      const float4 jlo = v.tile_box[2 * jt], jhi = v.tile_box[2 * jt + 1];
-      float gx = fmaxf(0.f, fmaxf(ilo.x - jhi.x, jlo.x - ihi.x));
-      float gy = fmaxf(0.f, fmaxf(ilo.y - jhi.y, jlo.y - ihi.y));
-      float gz = fmaxf(0.f, fmaxf(ilo.z - jhi.z, jlo.z - ihi.z));
-      if (gx * gx + gy * gy + gz * gz >= rc2) continue; /* warp-uniform */
-      const int j0 = a0 + 32 * (jt - tb);
-      const int j = j0 + lane;
-      f4 pj = j < a1 ? v.pos[j] : f4{0.f, 0.f, 0.f, 0.f};
-      int cj = j < a1 ? v.sclass[j] : -1;
-      for (int r = 0; r < 32; r++) {
-        if (r > 0) {
-          pj.x = __shfl_sync(0xffffffffu, pj.x, (lane + 1) & 31);
-          pj.y = __shfl_sync(0xffffffffu, pj.y, (lane + 1) & 31);
-          pj.z = __shfl_sync(0xffffffffu, pj.z, (lane + 1) & 31);
-          cj = __shfl_sync(0xffffffffu, cj, (lane + 1) & 31);
+  for (long long base = (long long)blockIdx.x * SF_BLOCK; base < v.natoms; base += (long long)gridDim.x * SF_BLOCK) {
+    const int g = (int)base + threadIdx.x;
+    if (g < v.natoms) {
+      for (int f = 0; f < SF_NF; f++) row[f] = 0.f;
+      const int I = v.inst_of[g];
+      const f4 pi = v.pos[g];
+      const int ci = v.sclass[g];
+      if (ci >= 0) sf_add(row, ci, 0.f);
+      int cx, cy, cz;
+      cell_of(pi.x, pi.y, pi.z, 1.0f / SF_RC, cx, cy, cz);
+      for (int c = 0; c < 27; c++) {
+        const int ax = cx + c % 3 - 1, ay = cy + (c / 3) % 3 - 1, az = cz + c / 9 - 1;
+        const int b = v.sf_bbegin[I] + cell_hash(ax, ay, az, v.sf_bmask[I]);
+        const int key = sf_key(ax, ay, az);
+        const int s0 = v.sf_bstart[b], s1 = s0 + v.sf_bcount[b];
+        for (int q = s0; q < s1; q++) {
+          const int2 id = v.sf_sid[q];
+          const f4 pj = v.sf_spos[q];
+          if (id.y != key || id.x == g || pj.w < 0.f) continue;
+          float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+          float d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 < rc2) sf_add(row, (int)pj.w, sqrtf(d2));
         }
-        const int jr = j0 + ((lane + r) & 31);
-        if (!vi || cj < 0 || jr == g) continue;
-        float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-        float d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 < rc2) sf_add(row, cj, sqrtf(d2));
       }
-    }
-    __syncwarp();
-    if (vi)
       for (int f = 0; f < SF_NF; f++) {
         float x = row[f];
         if (mean) x = (x - mean[f]) * invstd[f];
         out[(size_t)g * SF_NF + f] = __float2bfloat16(x);
       }
-    __syncwarp();
+    }
   }
 }
 
@@ -3064,17 +3073,24 @@ extern "C" int agb_dev_surrogate_classes(agb_dev *s, const double *class_radii, 
   return 0;
 }
 
-/* features of the coordinates of the last evaluation (internal order) */
+/* features of the coordinates of the last evaluation (internal order),
+   queued on the instance stream (which agbnp3_stream returns) */
 extern "C" int agb_dev_surrogate_features(agb_dev *s, const float *mean, const float *invstd, void *out) {
   CK(cudaSetDevice(s->device));
-  const int smem = 4 * 32 * (SF_NF + 1) * (int)sizeof(float);
-  CK(cudaFuncSetAttribute(k_sfeat, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_tile_box<<<nblocks(s->v.ntiles), BLK, 0, s->st>>>(s->v);
-  int grid = (s->v.ntiles + 3) / 4;
-  if (grid > 148 * 2) grid = 148 * 2;
-  if (grid < 1) grid = 1;
-  k_sfeat<<<grid, 128, smem, s->st>>>(s->v, mean, invstd, (__nv_bfloat16 *)out);
+  const int smem = SF_BLOCK * (SF_NF + 1) * (int)sizeof(float);
+  if (!s->sfeat_ready) {
+    CK(cudaFuncSetAttribute(k_sfeat, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    s->sfeat_ready = 1;
+  }
+  View &v = s->v;
+  CK(cudaMemsetAsync(v.sf_bcount, 0, sizeof(int) * v.sf_nbuckets, s->st));
+  CK(cudaMemsetAsync(v.sf_bcursor, 0, sizeof(int) * v.sf_nbuckets, s->st));
+  k_sf_cell_count<<<nblocks(s->natoms), BLK, 0, s->st>>>(v);
+  agb_scan_excl(v.sf_bcount, v.sf_bstart, v.sf_dc, v.sf_dc + 1, v.sf_nbuckets, s->scan_scratch, s->st);
+  k_sf_cell_fill<<<nblocks(s->natoms), BLK, 0, s->st>>>(v);
+  int grid = (s->natoms + SF_BLOCK - 1) / SF_BLOCK;
+  if (grid > 148 * 32) grid = 148 * 32;
+  k_sfeat<<<grid, SF_BLOCK, smem, s->st>>>(v, mean, invstd, (__nv_bfloat16 *)out);
   CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(s->st));
   return 0;
 }

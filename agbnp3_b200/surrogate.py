@@ -103,13 +103,15 @@ class Mlp:
     def _gemm(self, A, lda, B, ldb, bias, C, ldc, M, N, K):
         _ok(self.L.agbnp3_tc_gemm_async(_p(A), lda, _p(B), ldb, _p(bias), _p(C), ldc, M, N, K, self._s()), "tc_gemm")
 
-    def forward_batch(self, Xb, n):
-        """Y[:n] for bf16 inputs Xb [n, 160] (n <= B); keeps the activations"""
+    def forward_batch(self, Xb, n, train=False):
+        """Y[:n] for bf16 inputs Xb [n, 160] (n <= B); keeps the activations
+        (and, for training, their transposes)"""
         L, s, p = self.L, self._s(), self.p
+        h1t, h2t = (self.H1t, self.H2t) if train else (None, None)
         self._gemm(Xb, NIN, self.W1b, NIN, p["b1"], self.Z1, NH, n, NH, NIN)
-        _ok(L.agbnp3_mlp_act(_p(self.Z1), n, NH, NH, _p(self.H1), NH, _p(self.H1t), self.B, s), "act1")
+        _ok(L.agbnp3_mlp_act(_p(self.Z1), n, NH, NH, _p(self.H1), NH, _p(h1t), self.B, s), "act1")
         self._gemm(self.H1, NH, self.W2b, NH, p["b2"], self.Z2, NH, n, NH, NH)
-        _ok(L.agbnp3_mlp_act(_p(self.Z2), n, NH, NH, _p(self.H2), NH, _p(self.H2t), self.B, s), "act2")
+        _ok(L.agbnp3_mlp_act(_p(self.Z2), n, NH, NH, _p(self.H2), NH, _p(h2t), self.B, s), "act2")
         self._gemm(self.H2, NH, self.W3b, NH, p["b3"], self.Y, NOUT, n, NOUT, NH)
         return self.Y[:n]
 
@@ -120,7 +122,7 @@ class Mlp:
             self._alloc(B)
         _ok(L.agbnp3_mlp_gather(_p(X), _p(T), _p(idx), B, NIN, NOUT, _p(self.Xb), _p(self.Xt), B, _p(self.Tb), s),
             "gather")
-        self.forward_batch(self.Xb, B)
+        self.forward_batch(self.Xb, B, train=True)
         for v in self.g.values():
             v.zero_()
         self.loss.zero_()
@@ -165,18 +167,33 @@ class Mlp:
         self.pack()
 
 
-def classes_and_features(inst, natoms, mean=None, invstd=None):
-    """radial features (bf16 [natoms, 160], internal order) of the coordinates
-    of inst's last evaluation"""
+def set_classes(inst):
+    """assigns the atom classes from the radii; returns the unmatched count"""
     L = _bind()
     cr = (ctypes.c_double * len(CLASS_RADII))(*CLASS_RADII)
     un = ctypes.c_int(0)
     if L.agbnp3_surrogate_classes(inst.tag, cr, len(CLASS_RADII), ctypes.byref(un)) != AGBNP_OK:
         raise AGBNPError("agbnp3_surrogate_classes failed")
-    out = torch.empty(natoms, NIN, dtype=torch.bfloat16, device="cuda")
-    if L.agbnp3_surrogate_features(inst.tag, _p(mean), _p(invstd), _p(out)) != AGBNP_OK:
+    return un.value
+
+
+def features(inst, natoms, mean=None, invstd=None, out=None):
+    """radial features (bf16 [natoms, 160], internal order) of the coordinates
+    of inst's last evaluation, ordered before the work that torch's current
+    stream queues next"""
+    if out is None:
+        out = torch.empty(natoms, NIN, dtype=torch.bfloat16, device="cuda")
+    ist = torch.cuda.ExternalStream(inst.stream)
+    ist.wait_stream(torch.cuda.current_stream())
+    if _bind().agbnp3_surrogate_features(inst.tag, _p(mean), _p(invstd), _p(out)) != AGBNP_OK:
         raise AGBNPError("agbnp3_surrogate_features failed")
-    return un.value, out
+    torch.cuda.current_stream().wait_stream(ist)
+    return out
+
+
+def classes_and_features(inst, natoms, mean=None, invstd=None):
+    un = set_classes(inst)
+    return un, features(inst, natoms, mean, invstd)
 
 
 def labels(inst, natoms, system):
@@ -260,9 +277,105 @@ def predict_system(net, model, inst, natoms):
     return un, Y
 
 
+def born_radii(S, radius):
+    """Born radii from descreening sums as the engine computes them
+    (agbnp3.c:1174-1188): beta = 1/R - S/4pi, filtered to sqrt(0.02^2 + beta^2)"""
+    beta = 1.0 / radius - S / (4.0 * np.pi)
+    bf = np.where(beta < 0.0, 0.02, np.sqrt(0.02 ** 2 + beta ** 2))
+    return 1.0 / bf
+
+
+def gb_energy(system, int2ext, radii_b):
+    """GB energy (kcal/mol) of the system (internal order) at the given Born
+    radii, by the library's GB pair kernel (agbnp3_gb_energy_static)"""
+    L = lib()
+    vp = ctypes.c_void_p
+    L.agbnp3_gb_energy_static.argtypes = [ctypes.c_int] + [vp] * 5 + [ctypes.c_double] * 2 + [vp] * 3 + [vp]
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")  # noqa: E731
+    xyz = system.coords()[int2ext]
+    n = system.natoms
+    e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    dera = torch.zeros(n, dtype=torch.float64, device="cuda")
+    grad = torch.zeros(n, 3, dtype=torch.float64, device="cuda")
+    args = [d(xyz[:, 0]), d(xyz[:, 1]), d(xyz[:, 2]), d(np.asarray(system.charge)[int2ext]), d(radii_b)]
+    torch.cuda.synchronize()
+    rc = L.agbnp3_gb_energy_static(n, *(_p(a) for a in args), system.eps_in, system.eps_out, _p(e), _p(dera),
+                                   _p(grad), None)
+    if rc != AGBNP_OK:
+        raise AGBNPError("agbnp3_gb_energy_static failed")
+    torch.cuda.synchronize()
+    return e.item()
+
+
+def gain(models, natoms, seed=1, tolerances=(0.0, 0.01, 0.03, 0.1, 0.3, float("inf"))):
+    """What the ensemble surrogate gains on one globule: for each tolerance of
+    the residual check (atoms whose two networks disagree by more than tol on
+    the descreening sum fall back to the exact sum), the fraction that falls
+    back, the relative error of the GB energy, and the modelled time of the
+    descreening stage (surrogate + the fallback's share of the exact stage)
+    against the exact stage alone."""
+    from . import PREC_MIXED
+    s = make_globule(natoms, seed)
+    int2ext, _ = s.internal_order()
+    radius = np.asarray(s.r)[int2ext]
+    inst = Instance(s, precision=PREC_FP64)
+    inst.ener()
+    exact = labels(inst, natoms, s)[:, 0]
+    # the exact stage's time, from the chosen (mixed) path
+    mixed = Instance(s, precision=PREC_MIXED)
+    mixed.ener()
+    mixed.stage_timing(True)
+    ts = []
+    for _ in range(5):
+        mixed.ener()
+        ts.append(mixed.stage_times()["invb"])
+    t_exact = float(np.median(ts))
+    mixed.close()
+    nets = [load_model(m, batch=max(4096, (natoms + 15) // 16 * 16)) for m in models]
+    means = [torch.as_tensor(m["fmean"], device="cuda") for m in models]
+    invs = [torch.as_tensor(m["finvstd"], device="cuda") for m in models]
+    set_classes(inst)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    preds = []
+    times = []
+    F = torch.empty(natoms, NIN, dtype=torch.bfloat16, device="cuda")
+    for rep in range(4):
+        e0.record()
+        preds = []
+        last = None
+        for net, m, mu, iv in zip(nets, models, means, invs):
+            if last is None or not (torch.equal(mu, last[0]) and torch.equal(iv, last[1])):
+                features(inst, natoms, mu, iv, out=F)  # shared by networks with one normalisation
+                last = (mu, iv)
+            Y = net.predict(F)[:, 0] * float(m["tstd"][0]) + float(m["tmean"][0])
+            preds.append(Y)
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    t_sur = float(np.median(times[1:]))
+    P = torch.stack(preds).cpu().numpy()
+    mean, spread = P.mean(0), np.abs(P[0] - P[1]) if len(P) > 1 else np.zeros(natoms)
+    e_exact = gb_energy(s, int2ext, born_radii(exact, radius))
+    rows = []
+    for tol in tolerances:
+        fall = spread > tol if np.isfinite(tol) else np.zeros(natoms, bool)
+        if tol == 0.0:
+            fall[:] = True
+        S = np.where(fall, exact, mean)
+        e = gb_energy(s, int2ext, born_radii(S, radius))
+        frac = float(fall.mean())
+        rows.append({"tolerance": tol, "fallback_fraction": frac, "egb_rel_err": abs(e - e_exact) / abs(e_exact),
+                     "modelled_ms": t_sur + frac * t_exact, "exact_ms": t_exact,
+                     "rms_sum_err": float(np.sqrt(((S - exact) ** 2).mean()))})
+    inst.close()
+    return {"natoms": natoms, "surrogate_ms": t_sur, "exact_stage_ms": t_exact, "egb": e_exact, "rows": rows}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["train", "evaluate"])
+    ap.add_argument("cmd", choices=["train", "evaluate", "gain"])
+    ap.add_argument("--models", nargs="*", default=[])
+    ap.add_argument("--seeds", type=int, nargs="*", default=[0])
     ap.add_argument("--out", default="surrogate_model.npz")
     ap.add_argument("--model", default="surrogate_model.npz")
     ap.add_argument("--conformations", type=int, default=2000)
@@ -274,9 +387,15 @@ def main():
     initialize()
     if a.cmd == "train":
         X, T = make_dataset(a.conformations, a.natoms)
-        model = train(X, T, epochs=a.epochs, seed=a.seed)
-        np.savez(a.out, **model)
-        print(f"saved {a.out}")
+        for sd in a.seeds:
+            model = train(X, T, epochs=a.epochs, seed=sd)
+            out = a.out.replace("{seed}", str(sd))
+            np.savez(out, **model)
+            print(f"saved {out}")
+    elif a.cmd == "gain":
+        import json
+        r = gain([dict(np.load(m)) for m in a.models], a.natoms)
+        print(json.dumps(r))
     else:
         model = dict(np.load(a.model))
         net = load_model(model)

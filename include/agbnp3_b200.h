@@ -131,7 +131,8 @@ int agbnp3_gb_energy_static(int natoms, const double *x, const double *y, const 
    a cosine cutoff at 8 A, plus the atom's own class at distance 0) as bf16
    [natoms][160] in the engine's internal order (heavy atoms first) into the
    device array `out`, each feature (x - mean) * invstd when both are given
-   (device arrays [160]).  No counterpart in the reference. */
+   (device arrays [160]); the work is queued on the instance's stream
+   (agbnp3_stream), without waiting.  No counterpart in the reference. */
 int agbnp3_surrogate_classes(int tag, const double *class_radii, int nclass, int *unmatched);
 int agbnp3_surrogate_features(int tag, const float *mean, const float *invstd, void *out);
 

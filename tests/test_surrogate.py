@@ -45,6 +45,7 @@ def _features(inst, natoms):
     assert L.agbnp3_surrogate_classes(inst.tag, cr, 5, ctypes.byref(un)) == A.AGBNP_OK
     out = torch.empty(natoms, 160, dtype=torch.bfloat16, device="cuda")
     assert L.agbnp3_surrogate_features(inst.tag, None, None, _p(out)) == A.AGBNP_OK
+    torch.cuda.synchronize()  # the features are queued on the instance's stream
     return un.value, out.float().cpu().numpy()
 
 
@@ -115,3 +116,23 @@ def test_surrogate_training_reduces_loss():
     t = T[ntr:, 0].cpu().numpy()
     e = Y[:, 0].cpu().numpy() - t
     assert np.sqrt((e ** 2).mean()) < 0.5 * t.std()
+
+
+@pytest.mark.gpu
+def test_surrogate_gain_and_fallback():
+    """What the trained ensemble gains: with tolerance 0 every atom falls back
+    to the plain descreening and the GB energy is the exact one; with an
+    infinite tolerance none does; in between the fallback fraction falls as
+    the tolerance grows.  The measured gain is printed."""
+    import json
+    from agbnp3_b200 import surrogate as SG
+    X, T = SG.make_dataset(conformations=12, natoms=1500, bases=3, log=lambda *a: None)
+    models = [SG.train(X, T, epochs=4, batch=1024, lr=2e-3, seed=sd, log=lambda *a: None) for sd in (0, 1)]
+    r = SG.gain(models, 3000, seed=11)
+    print(json.dumps(r))
+    rows = r["rows"]
+    assert rows[0]["fallback_fraction"] == 1.0 and rows[0]["egb_rel_err"] <= 1e-12
+    assert rows[-1]["fallback_fraction"] == 0.0
+    fr = [q["fallback_fraction"] for q in rows]
+    assert all(a >= b for a, b in zip(fr, fr[1:]))
+    assert r["surrogate_ms"] > 0 and r["exact_stage_ms"] > 0
