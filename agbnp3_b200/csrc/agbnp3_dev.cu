@@ -2064,6 +2064,8 @@ struct agb_dev {
   int graph_ok;
   int timing;
   cudaEvent_t ev[AGB_NSTAGE + 1];
+  cudaStream_t st2;                /* side stream of the water-site stage */
+  cudaEvent_t fork_ev, join_ev;    /* orders st2 against st */
   cudaEvent_t xev; /* orders the instance stream against a caller's stream */
   double stage_ms[AGB_NSTAGE];
   long long nlaunch;
@@ -2271,6 +2273,9 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   s->precision = d->precision;
   s->compat = d->compat;
   CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming));
   View &v = s->v;
   memset(&v, 0, sizeof(v));
   int N = d->natoms, NI = d->ninst, NW = d->nws;
@@ -2523,6 +2528,9 @@ extern "C" void agb_dev_destroy(agb_dev *s) {
   for (int k = 0; k < s->nallocs; k++) cudaFree(s->allocs[k]);
   for (int k = 0; k <= AGB_NSTAGE; k++)
     if (s->ev[k]) cudaEventDestroy(s->ev[k]);
+  if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+  if (s->join_ev) cudaEventDestroy(s->join_ev);
+  if (s->st2) cudaStreamDestroy(s->st2);
   if (s->xev) cudaEventDestroy(s->xev);
   cudaStreamDestroy(s->st);
   if (s->items) cudaFree(s->items);
@@ -2568,6 +2576,16 @@ static inline int sym_grid(int n) {
   int b = (n + 3) / 4;
   if (b > 148 * 16) b = 148 * 16;
   return b < 1 ? 1 : b;
+}
+
+/* the water-site stage on `stream` */
+template <typename R>
+static void launch_ws(agb_dev *s, const View &v, cudaStream_t stream) {
+  AGB_LAUNCH(k_ws_geom<R>, nblocks(s->nws), BLK, stream, v);
+  AGB_LAUNCH(k_ws_count27<R>, nblocks(27LL * s->nws), BLK, stream, v);
+  agb_scan_excl(v.ws_c27, v.ws_o27, v.dc + DC_W27, v.dc + DC_WSC, 27 * s->nws, s->scan_scratch, stream);
+  AGB_LAUNCH(k_ws_emit27<R>, nblocks(27LL * s->nws), BLK, stream, v);
+  AGB_LAUNCH(k_ws_free<R>, sym_grid(s->nws), 128, stream, v);
 }
 
 static void stage_mark(agb_dev *s, int k) {
@@ -2624,6 +2642,18 @@ static void launch_all(agb_dev *s) {
   AGB_LAUNCH(k_pack_sp<R>, nblocks(N), BLK, st, v);
   nl += 2;
   stage_mark(s, 4);
+  /* the water-site stage needs only positions and spe (ready after the
+     scaling factors) and writes only its own outputs, the HB gradient and
+     derh: in a captured evaluation it runs on a side stream beside the pair
+     stages and joins before the tree-derivative pass */
+  const bool side = !s->timing && s->nws > 0;
+  if (side) {
+    cudaEventRecord(s->fork_ev, st);
+    cudaStreamWaitEvent(s->st2, s->fork_ev, 0);
+    launch_ws<R>(s, v, s->st2);
+    cudaEventRecord(s->join_ev, s->st2);
+    nl += 4 + 3;
+  }
   int pgrid = s->nitems < 148 * 16 ? s->nitems : 148 * 16;
   int dgrid = s->nitems < 148 * 32 ? s->nitems : 148 * 32; /* 64-thread descreening blocks */
   AGB_LAUNCH(k_descreen_t<R>, dgrid, ITILE / 2, st, v, s->items, s->nitems, s->nch);
@@ -2646,12 +2676,10 @@ static void launch_all(agb_dev *s) {
   AGB_LAUNCH(k_gbders_post, nblocks(N), BLK, st, v);
   nl += 2;
   stage_mark(s, 7);
-  if (s->nws > 0) {
-    AGB_LAUNCH(k_ws_geom<R>, nblocks(s->nws), BLK, st, v);
-    AGB_LAUNCH(k_ws_count27<R>, nblocks(27LL * s->nws), BLK, st, v);
-    agb_scan_excl(v.ws_c27, v.ws_o27, v.dc + DC_W27, v.dc + DC_WSC, 27 * s->nws, s->scan_scratch, st);
-    AGB_LAUNCH(k_ws_emit27<R>, nblocks(27LL * s->nws), BLK, st, v);
-    AGB_LAUNCH(k_ws_free<R>, sym_grid(s->nws), 128, st, v);
+  if (side) {
+    cudaStreamWaitEvent(st, s->join_ev, 0);
+  } else if (s->nws > 0) {
+    launch_ws<R>(s, v, st);
     nl += 4 + 3;
   }
   stage_mark(s, 8);
