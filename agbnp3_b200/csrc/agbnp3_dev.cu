@@ -747,18 +747,23 @@ struct Tab<double> {
   static __device__ __forceinline__ const double4 *val(const View &v) { return v.tabv_d; }
 };
 
+/* the same with the interval index clamped to AGB_NA-1, whose record is all
+   zeros: beyond the table (a >= 20) the value and the derivative are 0
+   without a test */
 template <typename R>
-__device__ __forceinline__ R spline(const typename Tab<R>::T *tv, int slot, R xh) {
-  int k = (int)xh;
+__device__ __forceinline__ R spline_z(const typename Tab<R>::T *tv, int slot, R xh) {
+  int k = min((int)xh, AGB_NA - 1);
   R t = xh - R(k);
   typename Tab<R>::T c = Tab<R>::ld(tv + (size_t)slot * AGB_NA + k);
   return c.x + t * (c.y + t * (c.z + t * c.w));
 }
 
-/* value and derivative in t; REF: the reference's derivative, else exact */
+/* value and derivative in t; REF: the reference's derivative, else exact.
+   The interval index is clamped to AGB_NA-1 (an all-zero record), so
+   beyond the table both are 0. */
 template <typename R, bool REF>
 __device__ __forceinline__ R spline_d(const typename Tab<R>::T *tv, int slot, R xh, R &fph) {
-  int k = (int)xh;
+  int k = min((int)xh, AGB_NA - 1);
   R t = xh - R(k);
   typename Tab<R>::T c = Tab<R>::ld(tv + (size_t)slot * AGB_NA + k);
   R d0 = REF ? c.y + R(2) * c.w + R(2.0 / 3.0) * c.z : c.y;
@@ -870,7 +875,7 @@ __global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__
           for (int u = 0; u < 2; u++) {
             R dx = a.x - xg[u], dy = a.y - yg[u], dz = a.z - zg[u];
             R xh = p_sqrt(dx * dx + dy * dy + dz * dz) * a.rh;
-            if (xh < R(AGB_NA - 1) && j0 + t != g[u]) part[u] += b.w * spline<R>(tab, row[u] + b.t, xh);
+            if (xh < R(AGB_NA - 1) && j0 + t != g[u]) part[u] += b.w * spline_z<R>(tab, row[u] + b.t, xh);
           }
         }
         acc[0] += (double)part[0];
@@ -1289,15 +1294,13 @@ struct GbdP { /* i-side sums over one j tile */
 template <typename R, bool SEL, bool REF>
 __device__ __forceinline__ bool gbd_q4(const typename Tab<R>::T *tv, int slot, R d, R rhs, R &q, R &dq) {
   R xh = d * rhs;
-  bool in = xh < R(AGB_NA - 1);
-  if (SEL) {
+  if (SEL) { /* no range test: the clamped lookup gives 0 beyond the table */
     R fp;
-    R f = spline_d<R, REF>(tv, slot, in ? xh : R(0), fp);
-    q = in ? f : R(0);
-    dq = in ? fp * rhs : R(0);
+    q = spline_d<R, REF>(tv, slot, xh, fp);
+    dq = fp * rhs;
     return true;
   }
-  if (!in) return false;
+  if (!(xh < R(AGB_NA - 1))) return false;
   R fp;
   q = spline_d<R, REF>(tv, slot, xh, fp);
   dq = fp * rhs;
@@ -1310,8 +1313,10 @@ __device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &
   for (int r = 0; r < 32; r++) {
     if (r > 0) {
       J.x = rot1(J.x); J.y = rot1(J.y); J.z = rot1(J.z);
-      J.rh = rot1(J.rh); J.sp = rot1(J.sp);
       J.q2 = rot1(J.q2); J.ab = rot1(J.ab); J.t = rot1(J.t);
+      if (MODE != GBD_HX) { /* hydrogens do not descreen: no radius, sp, U, V of j */
+        J.rh = rot1(J.rh); J.sp = rot1(J.sp);
+      }
     }
     const int jr = j0 + ((lane + r) & 31);
     const bool jok = MODE != GBD_GEN || jr < a1;
@@ -1350,7 +1355,9 @@ __device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &
       J.fx = fma(-ht, dx, J.fx); J.fy = fma(-ht, dy, J.fy); J.fz = fma(-ht, dz, J.fz);
       J.vx = fma(-ut, dx, J.vx); J.vy = fma(-ut, dy, J.vy); J.vz = fma(-ut, dz, J.vz);
     }
-    J.U = rot1(J.U); J.V = rot1(J.V);
+    if (MODE != GBD_HX) {
+      J.U = rot1(J.U); J.V = rot1(J.V);
+    }
     J.fx = rot1(J.fx); J.fy = rot1(J.fy); J.fz = rot1(J.fz);
     J.vx = rot1(J.vx); J.vy = rot1(J.vy); J.vz = rot1(J.vz);
   }
