@@ -64,6 +64,8 @@ def lib():
         L.agbnp3_ener.restype = ctypes.c_int
         L.agbnp3_set_mode.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.agbnp3_get_mode.argtypes = [ctypes.c_int, _ip, _ip]
+        L.agbnp3_pair_order.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.agbnp3_batch_pair_order.argtypes = [ctypes.c_int, ctypes.c_int]
         L.agbnp3_set_device.argtypes = [ctypes.c_int]
         L.agbnp3_set_coords.argtypes = [ctypes.c_int, _dp, _dp, _dp]
         L.agbnp3_ener_resident.argtypes = [ctypes.c_int]
@@ -207,6 +209,11 @@ class Instance:
     def set_mode(self, precision: int, compat: bool = True):
         _check(lib().agbnp3_set_mode(self.tag, int(precision), int(compat)), "agbnp3_set_mode")
 
+    def pair_order(self, mode: int = 1):
+        """1: pair passes over Hilbert-sorted atoms, taken from the next
+        evaluation's coordinates; 0: the internal order"""
+        _check(lib().agbnp3_pair_order(self.tag, int(mode)), "agbnp3_pair_order")
+
     def ener(self, xyz=None) -> dict:
         xyz = self.system.coords() if xyz is None else np.asarray(xyz)
         return ener(self.tag, xyz[:, 0], xyz[:, 1], xyz[:, 2])
@@ -278,6 +285,11 @@ class Instance:
         a, _ = self.debug_fetch(100 + k, self.natoms, np.float64)
         return a[: self.natoms]
 
+    def pair_slots(self):
+        """internal atom held by each pair slot"""
+        a, _ = self.debug_fetch(202, self.natoms)
+        return a[: self.natoms]
+
     def autotune(self) -> dict:
         """Times the pair-stage work decompositions at the current device
         coordinates and keeps the fastest (agbnp3_autotune)."""
@@ -309,6 +321,9 @@ class Batch:
 
     def set_mode(self, precision: int, compat: bool = True):
         _check(lib().agbnp3_batch_set_mode(self.btag, int(precision), int(compat)), "agbnp3_batch_set_mode")
+
+    def pair_order(self, mode: int = 1):
+        _check(lib().agbnp3_batch_pair_order(self.btag, int(mode)), "agbnp3_batch_pair_order")
 
     def set_coords(self, xyz):
         xyz = np.asarray(xyz, dtype=np.float64)

@@ -37,6 +37,7 @@
 
 #include <cuda_bf16.h>
 
+#include <cmath>
 #include <float.h>
 #include <limits.h>
 #include <math.h>
@@ -105,7 +106,12 @@ struct View {
   double *wsp;                        /* [nws] */
   double *o_sp, *o_br, *o_sa, *o_gb, *o_gv, *o_gc, *o_gh;
   int nbuckets;
-  void *pa[12];      /* packed pair-stage operands (R[natoms] each) */
+  void *pa[12];      /* packed operands (R[natoms] each); the pair-stage ones in slot order */
+  /* pair-stage slot order: each instance's heavy atoms, then its hydrogens,
+     each group sorted along a Hilbert curve so that 32 consecutive slots
+     are a compact cluster (identity until the first evaluation sets it) */
+  const int *slot_atom, *atom_slot;
+  int *slot_type; /* radius type by slot */
   int *nl_c27, *nl_o27; /* near-list counts / offsets per (atom, neighbour cell) */
   int *nl_tmp, *nl_own; /* unsorted entries and their atom */
   int *ws_c27, *ws_o27, *ws_cand; /* water-site candidates per (site, cell) */
@@ -135,7 +141,9 @@ enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m
 enum { F_A = 0, F_P, F_CX, F_CY, F_CZ, F_GVOL, F_GVOLP, F_FP, F_FPP, F_NUM = 12 };
 
 /* packed per-atom operands, in the working precision: position, 1/R,
-   1/(h R), Gaussian exponent KFC/R^2, sp, charge, B, 1/B, q2ab, abrw */
+   1/(h R), Gaussian exponent KFC/R^2, sp, charge, B, 1/B, q2ab, abrw.
+   1/R and the exponent (the overlap tree's) are indexed by atom; the pair
+   stages' operands by pair slot (View::atom_slot) */
 enum { PA_X = 0, PA_Y, PA_Z, PA_RINV, PA_RH, PA_SP, PA_ALPHA, PA_Q, PA_B, PA_BINV, PA_Q2AB, PA_ABRW, PA_NUM };
 
 template <typename R>
@@ -776,13 +784,15 @@ template <typename R>
 __global__ void k_pack_geom(View v) {
   AGB_GRID_STRIDE(g, v.natoms) {
     R ri = R(1) / (R)v.r[g];
-    pa<R>(v, PA_X)[g] = px<R>(v, (int)g);
-    pa<R>(v, PA_Y)[g] = py<R>(v, (int)g);
-    pa<R>(v, PA_Z)[g] = pz<R>(v, (int)g);
+    const int s = v.atom_slot[g];
+    pa<R>(v, PA_X)[s] = px<R>(v, (int)g);
+    pa<R>(v, PA_Y)[s] = py<R>(v, (int)g);
+    pa<R>(v, PA_Z)[s] = pz<R>(v, (int)g);
     pa<R>(v, PA_RINV)[g] = ri;
-    pa<R>(v, PA_RH)[g] = ri * R((AGB_NA - 1) / C_AMAX);
+    pa<R>(v, PA_RH)[s] = ri * R((AGB_NA - 1) / C_AMAX);
     pa<R>(v, PA_ALPHA)[g] = R(C_KFC) / ((R)v.r[g] * (R)v.r[g]);
-    pa<R>(v, PA_Q)[g] = (R)v.charge[g];
+    pa<R>(v, PA_Q)[s] = (R)v.charge[g];
+    v.slot_type[s] = v.rtype[g];
     v.acc_beta[g] = 0.0;
   }
 }
@@ -791,7 +801,7 @@ template <typename R>
 __global__ void k_pack_sp(View v) {
   AGB_GRID_STRIDE(g, v.natoms) {
     R sp = (R)v.sp[g];
-    pa<R>(v, PA_SP)[g] = sp;
+    pa<R>(v, PA_SP)[v.atom_slot[g]] = sp;
   }
 }
 
@@ -846,7 +856,7 @@ __global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__
       xg[u] = act[u] ? X[g[u]] : R(0);
       yg[u] = act[u] ? Y[g[u]] : R(0);
       zg[u] = act[u] ? Z[g[u]] : R(0);
-      row[u] = act[u] ? v.rtype[g[u]] * nt : 0;
+      row[u] = act[u] ? v.slot_type[g[u]] * nt : 0;
     }
     int p0 = v.inst_begin[w.x], c0, c1;
     chunk_range(p0, p0 + v.inst_nheavy[w.x], w.w, nch, c0, c1);
@@ -862,7 +872,7 @@ __global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__
         sp4[t] = a;
         PartW<R> b;
         b.w = W[j0 + t];
-        b.t = v.rtype[j0 + t];
+        b.t = v.slot_type[j0 + t];
         spw[t] = b;
       }
       AGB_SYNC();
@@ -884,7 +894,7 @@ __global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__
     }
 #pragma unroll
     for (int u = 0; u < 2; u++)
-      if (act[u]) atomicAdd(&v.acc_beta[g[u]], acc[u]);
+      if (act[u]) atomicAdd(&v.acc_beta[v.slot_atom[g[u]]], acc[u]);
   }
 }
 
@@ -914,8 +924,8 @@ __global__ void k_born(View v) {
     v.eatom[3 * N + g] = v.salpha[g] * a3;
     v.eatom[N + g] = 0.0;
     v.dera[g] = 0.0;
-    pa<R>(v, PA_B)[g] = (R)b;
-    pa<R>(v, PA_BINV)[g] = (R)bf;
+    pa<R>(v, PA_B)[v.atom_slot[g]] = (R)b;
+    pa<R>(v, PA_BINV)[v.atom_slot[g]] = (R)bf;
   }
 }
 
@@ -977,12 +987,13 @@ __global__ void __launch_bounds__(ITILE) k_agb_t(View v, const int4 *__restrict_
     }
     if (act) {
       /* qj and the factor 2 df qi are applied once per atom */
-      double qi = v.charge[g], w2 = 2.0 * df * qi;
-      atomicAdd(&v.eatom[N + g], C_TOKCAL * 0.5 * w2 * e);
-      atomicAdd(&v.g_gb[3 * g], w2 * gx);
-      atomicAdd(&v.g_gb[3 * g + 1], w2 * gy);
-      atomicAdd(&v.g_gb[3 * g + 2], w2 * gz);
-      atomicAdd(&v.dera[g], qi * at);
+      const int ga = v.slot_atom[g];
+      double qi = v.charge[ga], w2 = 2.0 * df * qi;
+      atomicAdd(&v.eatom[N + ga], C_TOKCAL * 0.5 * w2 * e);
+      atomicAdd(&v.g_gb[3 * ga], w2 * gx);
+      atomicAdd(&v.g_gb[3 * ga + 1], w2 * gy);
+      atomicAdd(&v.g_gb[3 * ga + 2], w2 * gz);
+      atomicAdd(&v.dera[ga], qi * at);
     }
   }
 }
@@ -998,8 +1009,8 @@ __global__ void k_agb_post(View v) {
     double abrw = (v.ialpha[g] + v.salpha[g]) * v.brw[g] * v.bder[g];
     v.q2ab[g] = q2ab;
     v.abrw[g] = abrw;
-    pa<R>(v, PA_Q2AB)[g] = (R)q2ab;
-    pa<R>(v, PA_ABRW)[g] = (R)abrw;
+    pa<R>(v, PA_Q2AB)[v.atom_slot[g]] = (R)q2ab;
+    pa<R>(v, PA_ABRW)[v.atom_slot[g]] = (R)abrw;
     v.deru[g] = v.derv[g] = 0.0;
   }
 }
@@ -1013,14 +1024,13 @@ __global__ void k_agb_post(View v) {
 template <typename R>
 __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restrict__ items, int nitems,
                                                     int nch) {
-  AGB_SHARED R sx[ITILE], sy[ITILE], sz[ITILE], srh[ITILE], sri[ITILE], ssp[ITILE], sq2[ITILE], sab[ITILE];
+  AGB_SHARED R sx[ITILE], sy[ITILE], sz[ITILE], srh[ITILE], ssp[ITILE], sq2[ITILE], sab[ITILE];
   AGB_SHARED int st[ITILE];
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
-  const R *RH = pa<R>(v, PA_RH), *RI = pa<R>(v, PA_RINV), *SP = pa<R>(v, PA_SP);
+  const R *RH = pa<R>(v, PA_RH), *SP = pa<R>(v, PA_SP);
   const R *Q2 = pa<R>(v, PA_Q2AB), *AB = pa<R>(v, PA_ABRW);
   const typename Tab<R>::T *tv = Tab<R>::val(v);
   const bool ref = v.compat != 0;
-  const R hinv = R((AGB_NA - 1) / C_AMAX);
   const int nt = v.ntypes;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     int4 w = items[it];
@@ -1032,9 +1042,9 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
     chunk_range(a0, w.y >= hh ? hh : a1, w.w, nch, c0, c1);
     bool heavy = g < hh;
     R xg = act ? X[g] : R(0), yg = act ? Y[g] : R(0), zg = act ? Z[g] : R(0);
-    R rhg = act ? RH[g] : R(0), rig = act ? RI[g] : R(0), spg = act ? SP[g] : R(0);
+    R rhg = act ? RH[g] : R(0), spg = act ? SP[g] : R(0);
     R q2g = act ? Q2[g] : R(0), abg = act ? AB[g] : R(0);
-    int tg = act ? v.rtype[g] : 0;
+    int tg = act ? v.slot_type[g] : 0;
     double U = 0, V = 0, fx = 0, fy = 0, fz = 0, vx = 0, vy = 0, vz = 0;
     for (int j0 = c0; j0 < c1; j0 += ITILE) {
       int n = min(ITILE, c1 - j0);
@@ -1044,11 +1054,10 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
         sy[t] = Y[j0 + t];
         sz[t] = Z[j0 + t];
         srh[t] = RH[j0 + t];
-        sri[t] = RI[j0 + t];
         ssp[t] = SP[j0 + t];
         sq2[t] = Q2[j0 + t];
         sab[t] = AB[j0 + t];
-        st[t] = v.rtype[j0 + t];
+        st[t] = v.slot_type[j0 + t];
       }
       AGB_SYNC();
       if (act) {
@@ -1067,7 +1076,7 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
             if (xh < R(AGB_NA - 1)) {
               R fp;
               R f = ref ? spline_d<R, true>(tv, st[t] * nt + tg, xh, fp) : spline_d<R, false>(tv, st[t] * nt + tg, xh, fp);
-              R q = f, dq = fp * hinv * rig;
+              R q = f, dq = fp * rhg;
               pu += sq2[t] * q;
               pv += sab[t] * q;
               ht += sq2[t] * dq * spg;
@@ -1082,7 +1091,7 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
                 spline_d<R, true>(tv, tg * nt + st[t], xh, fp);
               else
                 spline_d<R, false>(tv, tg * nt + st[t], xh, fp);
-              R dq = fp * hinv * sri[t] * ssp[t];
+              R dq = fp * srh[t] * ssp[t];
               ht += q2g * dq;
               ut += abg * dq;
             }
@@ -1109,15 +1118,16 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
     if (act) {
       const double f4p = 1.0 / (4.0 * C_PI);
       double kg = f4p * v.inst_df[w.x];
-      atomicAdd(&v.g_gb[3 * g], kg * fx);
-      atomicAdd(&v.g_gb[3 * g + 1], kg * fy);
-      atomicAdd(&v.g_gb[3 * g + 2], kg * fz);
-      atomicAdd(&v.g_vw[3 * g], f4p * vx);
-      atomicAdd(&v.g_vw[3 * g + 1], f4p * vy);
-      atomicAdd(&v.g_vw[3 * g + 2], f4p * vz);
+      const int ga = v.slot_atom[g];
+      atomicAdd(&v.g_gb[3 * ga], kg * fx);
+      atomicAdd(&v.g_gb[3 * ga + 1], kg * fy);
+      atomicAdd(&v.g_gb[3 * ga + 2], kg * fz);
+      atomicAdd(&v.g_vw[3 * ga], f4p * vx);
+      atomicAdd(&v.g_vw[3 * ga + 1], f4p * vy);
+      atomicAdd(&v.g_vw[3 * ga + 2], f4p * vz);
       if (heavy) {
-        atomicAdd(&v.deru[g], U);
-        atomicAdd(&v.derv[g], V);
+        atomicAdd(&v.deru[ga], U);
+        atomicAdd(&v.derv[ga], V);
       }
     }
   }
@@ -1244,16 +1254,17 @@ __global__ void __launch_bounds__(128) k_agb_sym(View v, const int4 *__restrict_
       else
         agb_tile<R, false>(I, J, P, lane, j0, a1);
       if (vj) {
-        atomicAdd(&v.g_gb[3 * j], w2 * (double)J.gx);
-        atomicAdd(&v.g_gb[3 * j + 1], w2 * (double)J.gy);
-        atomicAdd(&v.g_gb[3 * j + 2], w2 * (double)J.gz);
-        atomicAdd(&v.dera[j], (double)J.at);
+        const int ja = v.slot_atom[j];
+        atomicAdd(&v.g_gb[3 * ja], w2 * (double)J.gx);
+        atomicAdd(&v.g_gb[3 * ja + 1], w2 * (double)J.gy);
+        atomicAdd(&v.g_gb[3 * ja + 2], w2 * (double)J.gz);
+        atomicAdd(&v.dera[ja], (double)J.at);
       }
     }
 #pragma unroll
     for (int u = 0; u < AGB_NI; u++) {
-      int i = I.ia[u];
-      if (i >= a1) continue;
+      if (I.ia[u] >= a1) continue;
+      const int i = v.slot_atom[I.ia[u]];
       atomicAdd(&v.eatom[N + i], C_TOKCAL * w2 * (double)P.e[u]);
       atomicAdd(&v.g_gb[3 * i], w2 * (double)P.gx[u]);
       atomicAdd(&v.g_gb[3 * i + 1], w2 * (double)P.gy[u]);
@@ -1326,13 +1337,18 @@ __device__ __forceinline__ void gbd_tile(const GbdI<R> &I, GbdJ<R> &J, GbdP<R> &
       const bool hiu = MODE != GBD_GEN || I.hi[u];
       R dx = J.x - I.x[u], dy = J.y - I.y[u], dz = J.z - I.z[u];
       R d2 = dx * dx + dy * dy + dz * dz;
-      if (MODE == GBD_GEN) {
-        if (!(jok && I.ia[u] < jr && (hiu || hj) && d2 > R(0))) continue;
-      } else if (!(d2 > R(0))) {
-        continue; /* coincident atoms */
-      }
       R id = p_rsqrt(d2);
       R d = d2 * id;
+      if (MODE == GBD_GEN) {
+        if (!(jok && I.ia[u] < jr && (hiu || hj) && d2 > R(0))) continue;
+      } else {
+        /* a step in which no lane's pair is inside the table in either
+           direction adds exactly zero: the warp skips it (the vote comes
+           before any lane leaves the step) */
+        const bool inr = d * I.rh[u] < R(AGB_NA - 1) || (MODE == GBD_HH && d * J.rh < R(AGB_NA - 1));
+        if (!__any_sync(0xffffffffu, inr)) continue;
+        if (!(d2 > R(0))) continue; /* coincident atoms */
+      }
       R ht = R(0), ut = R(0), q, dq;
       if (hiu && gbd_q4<R, MODE != GBD_GEN, REF>(tv, J.t * nt + I.ti[u], d, I.rh[u], q, dq)) {
         /* j descreened by i: table (type j, type i), radius of i */
@@ -1390,7 +1406,7 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       I.sp[u] = ok ? SP[i] : R(0);
       I.q2[u] = ok ? Q2[i] : R(0);
       I.ab[u] = ok ? AB[i] : R(0);
-      I.ti[u] = ok ? v.rtype[i] : 0;
+      I.ti[u] = ok ? v.slot_type[i] : 0;
       I.ia[u] = ok ? i : INT_MAX; /* no valid partner: i < j never holds */
       P.U[u] = P.V[u] = P.fx[u] = P.fy[u] = P.fz[u] = P.vx[u] = P.vy[u] = P.vz[u] = R(0);
     }
@@ -1407,7 +1423,7 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       J.sp = vj ? SP[j] : R(0);
       J.q2 = vj ? Q2[j] : R(0);
       J.ab = vj ? AB[j] : R(0);
-      J.t = vj ? v.rtype[j] : 0;
+      J.t = vj ? v.slot_type[j] : 0;
       J.U = J.V = J.fx = J.fy = J.fz = J.vx = J.vy = J.vz = R(0);
       /* warp-uniform tile class */
       const bool interior = iheavy && j0 >= w.y + 32 * GBD_NI;
@@ -1418,22 +1434,23 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
       else
         gbd_tile<R, GBD_GEN, REF>(I, J, P, lane, j0, a1, hh, tv, nt);
       if (vj) {
-        atomicAdd(&v.g_gb[3 * j], kg * (double)J.fx);
-        atomicAdd(&v.g_gb[3 * j + 1], kg * (double)J.fy);
-        atomicAdd(&v.g_gb[3 * j + 2], kg * (double)J.fz);
-        atomicAdd(&v.g_vw[3 * j], f4p * (double)J.vx);
-        atomicAdd(&v.g_vw[3 * j + 1], f4p * (double)J.vy);
-        atomicAdd(&v.g_vw[3 * j + 2], f4p * (double)J.vz);
+        const int ja = v.slot_atom[j];
+        atomicAdd(&v.g_gb[3 * ja], kg * (double)J.fx);
+        atomicAdd(&v.g_gb[3 * ja + 1], kg * (double)J.fy);
+        atomicAdd(&v.g_gb[3 * ja + 2], kg * (double)J.fz);
+        atomicAdd(&v.g_vw[3 * ja], f4p * (double)J.vx);
+        atomicAdd(&v.g_vw[3 * ja + 1], f4p * (double)J.vy);
+        atomicAdd(&v.g_vw[3 * ja + 2], f4p * (double)J.vz);
         if (j < hh) {
-          atomicAdd(&v.deru[j], (double)J.U);
-          atomicAdd(&v.derv[j], (double)J.V);
+          atomicAdd(&v.deru[ja], (double)J.U);
+          atomicAdd(&v.derv[ja], (double)J.V);
         }
       }
     }
 #pragma unroll
     for (int u = 0; u < GBD_NI; u++) {
-      int i = I.ia[u];
-      if (i >= a1) continue;
+      if (I.ia[u] >= a1) continue;
+      const int i = v.slot_atom[I.ia[u]];
       atomicAdd(&v.g_gb[3 * i], kg * (double)P.fx[u]);
       atomicAdd(&v.g_gb[3 * i + 1], kg * (double)P.fy[u]);
       atomicAdd(&v.g_gb[3 * i + 2], kg * (double)P.fz[u]);
@@ -2086,6 +2103,9 @@ struct agb_dev {
   int items_prec;  /* precision the symmetric items were built for (i block size) */
   int sfeat_ready; /* the feature kernel's shared-memory limit is set */
   int *h_inst_nheavy;
+  int *h_ext_of;  /* external index of each internal atom */
+  int pair_order; /* 1: pair slots along a Hilbert curve, 0: identity */
+  int order_ok;   /* the slot order is set for the current mode */
 };
 
 static int dev_alloc(agb_dev *s, void **p, size_t bytes) {
@@ -2470,6 +2490,20 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     v.pa[k] = p;
   }
   {
+    /* pair slots: the identity until the first evaluation orders them */
+    int *id = (int *)malloc(sizeof(int) * N);
+    for (int g = 0; g < N; g++) id[g] = g;
+    UP(slot_atom, id, N, int);
+    UP(atom_slot, id, N, int);
+    free(id);
+    DALLOC(v.slot_type, N, int);
+    s->h_ext_of = (int *)malloc(sizeof(int) * N);
+    memcpy(s->h_ext_of, d->ext_of, sizeof(int) * N);
+    const char *po = getenv("AGBNP3_PAIR_ORDER");
+    s->pair_order = po ? atoi(po) != 0 : 1;
+    s->order_ok = !s->pair_order;
+  }
+  {
     const char *tp = getenv("AGBNP3_PAIR_TILED");
     s->tiled_pairs = tp && atoi(tp) != 0;
     int nch = 0, jb = 8;
@@ -2546,7 +2580,136 @@ extern "C" void agb_dev_destroy(agb_dev *s) {
   free(s->h_inst_begin);
   free(s->h_ws_begin);
   free(s->h_inst_nheavy);
+  free(s->h_ext_of);
   free(s);
+}
+
+/* Hilbert index of a point of 3 coordinates of `bits` bits each: J. Skilling,
+   "Programming the Hilbert curve", AIP Conf. Proc. 707 (2004) -- the axes
+   are turned into the transposed index in place, whose bits are then
+   interleaved, most significant first. */
+static unsigned long long hilbert3(unsigned int X[3], int bits) {
+  const unsigned int M = 1u << (bits - 1);
+  for (unsigned int Q = M; Q > 1; Q >>= 1) {
+    const unsigned int P = Q - 1;
+    for (int i = 0; i < 3; i++) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        unsigned int t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  for (int i = 1; i < 3; i++) X[i] ^= X[i - 1];
+  unsigned int t = 0;
+  for (unsigned int Q = M; Q > 1; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1;
+  for (int i = 0; i < 3; i++) X[i] ^= t;
+  unsigned long long h = 0;
+  for (int b = bits - 1; b >= 0; b--)
+    for (int i = 0; i < 3; i++) h = (h << 1) | ((X[i] >> b) & 1u);
+  return h;
+}
+
+struct slot_key {
+  unsigned long long key;
+  int g;
+};
+static int slot_key_cmp(const void *a, const void *b) {
+  const slot_key *p = (const slot_key *)a, *q = (const slot_key *)b;
+  if (p->key != q->key) return p->key < q->key ? -1 : 1;
+  return (p->g > q->g) - (p->g < q->g);
+}
+
+/* Pair slots from the coordinates staged for the next evaluation: within
+   each instance the heavy atoms keep slots [begin, begin + nheavy) and the
+   hydrogens the rest, each group sorted by the Hilbert index of its atoms
+   on a 2^10 grid over the instance's bounding cube (ties by atom).  The
+   order only changes which atoms share a 32-atom tile of the pair passes
+   (and so the summation order); any order gives the same pairs. */
+static int order_pair_slots(agb_dev *s) {
+  const int N = s->natoms;
+  CK(cudaStreamSynchronize(s->st));
+  double *xyz = (double *)malloc(sizeof(double) * 3 * (size_t)N);
+  int *sa = (int *)malloc(sizeof(int) * N), *as = (int *)malloc(sizeof(int) * N);
+  slot_key *keys = (slot_key *)malloc(sizeof(slot_key) * N);
+  if (!xyz || !sa || !as || !keys) {
+    free(xyz); free(sa); free(as); free(keys);
+    FAIL("out of host memory");
+  }
+  int rc = 0;
+  if (cudaMemcpy(xyz, s->v.x_ext, sizeof(double) * N, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(xyz + N, s->v.y_ext, sizeof(double) * N, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(xyz + 2 * (size_t)N, s->v.z_ext, sizeof(double) * N, cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = -1;
+  const int bits = 10, top = (1 << bits) - 1;
+  for (int I = 0; I < s->ninst && rc == 0; I++) {
+    const int a0 = s->h_inst_begin[I], hh = a0 + s->h_inst_nheavy[I], a1 = s->h_inst_begin[I + 1];
+    double lo[3] = {0.0, 0.0, 0.0}, hi[3] = {0.0, 0.0, 0.0};
+    bool first = true;
+    for (int g = a0; g < a1; g++) {
+      double p[3];
+      for (int c = 0; c < 3; c++) p[c] = xyz[(size_t)c * N + s->h_ext_of[g]];
+      if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) continue;
+      for (int c = 0; c < 3; c++) {
+        if (first || p[c] < lo[c]) lo[c] = p[c];
+        if (first || p[c] > hi[c]) hi[c] = p[c];
+      }
+      first = false;
+    }
+    double ext = fmax(hi[0] - lo[0], fmax(hi[1] - lo[1], hi[2] - lo[2]));
+    const double sc = ext > 0.0 ? top / ext : 0.0;
+    const int grp[3] = {a0, hh, a1};
+    for (int k = 0; k < 2; k++) {
+      int n = 0;
+      for (int g = grp[k]; g < grp[k + 1]; g++) {
+        unsigned int X[3];
+        for (int c = 0; c < 3; c++) {
+          double q = (xyz[(size_t)c * N + s->h_ext_of[g]] - lo[c]) * sc;
+          X[c] = q >= 0.0 && q <= (double)top ? (unsigned int)q : (q > (double)top ? (unsigned int)top : 0u);
+        }
+        keys[n].key = hilbert3(X, bits);
+        keys[n].g = g;
+        n++;
+      }
+      qsort(keys, n, sizeof(slot_key), slot_key_cmp);
+      for (int q = 0; q < n; q++) {
+        sa[grp[k] + q] = keys[q].g;
+        as[keys[q].g] = grp[k] + q;
+      }
+    }
+  }
+  if (rc == 0 && (upload((void *)s->v.slot_atom, sa, sizeof(int) * N) ||
+                  upload((void *)s->v.atom_slot, as, sizeof(int) * N)))
+    rc = -1;
+  free(xyz); free(sa); free(as); free(keys);
+  if (rc) FAIL("pair slot order: %s", cudaGetErrorString(cudaGetLastError()));
+  s->order_ok = 1;
+  return 0;
+}
+
+/* mode 1: order the pair slots along a Hilbert curve from the coordinates
+   of the next evaluation (again on each call); mode 0: the identity */
+extern "C" int agb_dev_set_pair_order(agb_dev *s, int mode) {
+  CK(cudaSetDevice(s->device));
+  if (mode != 0 && mode != 1) FAIL("unknown pair order %d", mode);
+  s->pair_order = mode;
+  if (mode == 1) {
+    s->order_ok = 0;
+    return 0;
+  }
+  CK(cudaStreamSynchronize(s->st));
+  int *id = (int *)malloc(sizeof(int) * s->natoms);
+  if (!id) FAIL("out of host memory");
+  for (int g = 0; g < s->natoms; g++) id[g] = g;
+  int rc = upload((void *)s->v.slot_atom, id, sizeof(int) * s->natoms) ||
+           upload((void *)s->v.atom_slot, id, sizeof(int) * s->natoms);
+  free(id);
+  if (rc) return -1;
+  s->order_ok = 1;
+  return 0;
 }
 
 extern "C" int agb_dev_set_mode(agb_dev *s, int precision, int compat) {
@@ -2745,6 +2908,7 @@ static int run_once(agb_dev *s) {
 
 extern "C" int agb_dev_evaluate(agb_dev *s) {
   CK(cudaSetDevice(s->device));
+  if (!s->order_ok && order_pair_slots(s)) return -1;
   /* each attempt can reveal the overflow of one more buffer (a level's
      size is only known once the level below fits) */
   for (int attempt = 0; attempt < 16; attempt++) {
@@ -2855,6 +3019,7 @@ enum {
   DBG_ATOM = 100,   /* + k: double[natoms] per-atom array k */
   DBG_WS_SP = 200,  /* double[nws] */
   DBG_WS_POS,       /* double[3*nws] */
+  DBG_SLOT_ATOM,    /* int[natoms]: the atom in each pair slot */
 };
 
 extern "C" long long agb_dev_debug_fetch(agb_dev *s, int what, void *out, long long cap) {
@@ -2888,6 +3053,11 @@ extern "C" long long agb_dev_debug_fetch(agb_dev *s, int what, void *out, long l
     int k = what - DBG_ATOM;
     if (k >= (int)(sizeof(arrs) / sizeof(arrs[0])) || cap < N) return -1;
     cudaMemcpy(out, arrs[k], sizeof(double) * N, cudaMemcpyDeviceToHost);
+    return N;
+  }
+  if (what == DBG_SLOT_ATOM) {
+    if (cap < N) return -1;
+    cudaMemcpy(out, v.slot_atom, sizeof(int) * N, cudaMemcpyDeviceToHost);
     return N;
   }
   if (what == DBG_WS_SP) {

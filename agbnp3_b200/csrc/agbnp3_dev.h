@@ -87,6 +87,9 @@ int agb_dev_upload_coords(agb_dev *s, const double *x, const double *y, const do
    the device.  Returns 0, or a negative error after checking the device
    error word (capacities are grown and the evaluation repeated on overflow). */
 int agb_dev_evaluate(agb_dev *s);
+/* pair-stage slot order: 1 = along a Hilbert curve (set from the
+   coordinates of the next evaluation), 0 = identity */
+int agb_dev_set_pair_order(agb_dev *s, int mode);
 /* device -> host copies of the outputs of the last evaluation (any pointer
    may be NULL).  energies: [ninst][7] egb evdw ecorr_vdw ecav ecorr_cav ehb
    mol_volume.  Gradients are AoS [natoms][3], external order. */

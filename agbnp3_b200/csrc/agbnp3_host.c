@@ -728,6 +728,16 @@ int agbnp3_set_mode(int tag, int precision, int compat) {
   return AGBNP_OK;
 }
 
+int agbnp3_pair_order(int tag, int mode) {
+  inst_t *I = get_inst(tag, "agbnp3_pair_order()");
+  if (!I) return AGBNP_ERR;
+  if (agb_dev_set_pair_order(I->dev, mode) != 0) {
+    errprint("agbnp3_pair_order(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  return AGBNP_OK;
+}
+
 int agbnp3_get_mode(int tag, int *precision, int *compat) {
   inst_t *I = get_inst(tag, "agbnp3_get_mode()");
   if (!I) return AGBNP_ERR;
@@ -994,6 +1004,16 @@ int agbnp3_batch_set_mode(int btag, int precision, int compat) {
   }
   B->precision = precision;
   B->compat = compat;
+  return AGBNP_OK;
+}
+
+int agbnp3_batch_pair_order(int btag, int mode) {
+  batch_t *B = get_batch(btag, "agbnp3_batch_pair_order()");
+  if (!B) return AGBNP_ERR;
+  if (agb_dev_set_pair_order(B->dev, mode) != 0) {
+    errprint("agbnp3_batch_pair_order(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
   return AGBNP_OK;
 }
 

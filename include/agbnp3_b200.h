@@ -26,6 +26,19 @@ extern "C" {
 int agbnp3_set_mode(int tag, int precision, int compat);
 int agbnp3_get_mode(int tag, int *precision, int *compat);
 
+/* Order of the atoms inside the pair passes (no counterpart in the
+   reference, whose pair loops run in its internal order).  mode 1 (the
+   default; $AGBNP3_PAIR_ORDER=0 changes it): each instance's heavy atoms and
+   its hydrogens are each sorted along a Hilbert curve, so that 32
+   consecutive atoms form a compact cluster and a warp can skip the
+   rotation steps whose pairs all lie beyond the Q4 tables' range (about a
+   quarter of them in a 25,000-atom globule); the order is taken from the
+   coordinates of the next evaluation and kept until this is called again
+   (an MD caller may call it every few thousand steps).  mode 0: the
+   internal order.  The order changes no pair and no result beyond the
+   summation order of the pair sums. */
+int agbnp3_pair_order(int tag, int mode);
+
 /* CUDA device used by instances created afterwards (default: $AGBNP3_DEVICE,
    else $LOCAL_RANK, else 0) */
 int agbnp3_set_device(int device);
@@ -95,6 +108,8 @@ int agbnp3_batch_ener_resident(int btag);
 int agbnp3_batch_get_results(int btag, double *energies, double *sp, double *br, double *surf_area,
                              double (*dgbdr)[3], double (*dvwdr)[3], double (*decav)[3], double (*dehb)[3]);
 int agbnp3_batch_set_mode(int btag, int precision, int compat);
+/* agbnp3_pair_order for a batch (every member's atoms ordered separately) */
+int agbnp3_batch_pair_order(int btag, int mode);
 /* agbnp3_ener_device for a batch: arrays span all members, concatenated
    in member order; energies [7 * members] */
 int agbnp3_batch_ener_device(int btag, const double *x, const double *y, const double *z, double *energies,

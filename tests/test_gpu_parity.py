@@ -330,3 +330,42 @@ def test_one_sided_pair_kernels(engine, monkeypatch, prec):
     finally:
         inst.close()
         base.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+def test_pair_slot_order(engine, prec):
+    """Hilbert-ordered pair slots (the default) against the internal order:
+    the slots are a permutation that keeps the heavy atoms ahead of the
+    hydrogens; both orders give the oracle's results and agree with each
+    other up to summation order; after the atoms move, ordering again
+    changes the slots and the results stay right."""
+    s, _ = load_golden("globule2000_hbmix")
+    q = O.oracle_eval(s)
+    n, nh = s.natoms, s.nheavy
+    inst = A.Instance(s, precision=prec)
+    try:
+        r1 = inst.ener()
+        slots = inst.pair_slots()
+        assert np.array_equal(np.sort(slots), np.arange(n))
+        assert (slots[:nh] < nh).all()
+        assert not np.array_equal(slots, np.arange(n))
+        check_vs_oracle(r1, q, prec, "hilbert")
+        inst.pair_order(0)
+        r0 = inst.ener()
+        assert np.array_equal(inst.pair_slots(), np.arange(n))
+        check_vs_oracle(r0, q, prec, "identity")
+        tol = 1e-11 if prec == A.PREC_FP64 else 1e-5
+        for k in ENERGY_KEYS:
+            assert abs(r1[k] - r0[k]) <= tol * max(abs(r0[k]), 10.0), (k, r1[k], r0[k])
+        for k in ("br", "dgbdr", "dvwdr"):
+            assert rms_rel(r1[k], r0[k]) <= 10 * tol, (k, rms_rel(r1[k], r0[k]))
+        rng = np.random.default_rng(11)
+        xyz = s.coords() + rng.normal(0.0, 0.5, (n, 3))
+        s2 = s.with_coords(xyz)
+        inst.pair_order(1)
+        r2 = inst.ener(s2.coords())
+        slots2 = inst.pair_slots()
+        assert np.array_equal(np.sort(slots2), np.arange(n)) and not np.array_equal(slots2, slots)
+        check_vs_oracle(r2, O.oracle_eval(s2), prec, "reordered")
+    finally:
+        inst.close()
