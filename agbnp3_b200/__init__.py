@@ -66,6 +66,8 @@ def lib():
         L.agbnp3_get_mode.argtypes = [ctypes.c_int, _ip, _ip]
         L.agbnp3_pair_order.argtypes = [ctypes.c_int, ctypes.c_int]
         L.agbnp3_batch_pair_order.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.agbnp3_set_nblist_skin.argtypes = [ctypes.c_int, ctypes.c_double]
+        L.agbnp3_batch_set_nblist_skin.argtypes = [ctypes.c_int, ctypes.c_double]
         L.agbnp3_set_device.argtypes = [ctypes.c_int]
         L.agbnp3_set_coords.argtypes = [ctypes.c_int, _dp, _dp, _dp]
         L.agbnp3_ener_resident.argtypes = [ctypes.c_int]
@@ -214,6 +216,10 @@ class Instance:
         evaluation's coordinates; 0: the internal order"""
         _check(lib().agbnp3_pair_order(self.tag, int(mode)), "agbnp3_pair_order")
 
+    def set_nblist_skin(self, skin: float):
+        """Verlet skin (A) of the near list; 0 searches it at every evaluation"""
+        _check(lib().agbnp3_set_nblist_skin(self.tag, float(skin)), "agbnp3_set_nblist_skin")
+
     def ener(self, xyz=None) -> dict:
         xyz = self.system.coords() if xyz is None else np.asarray(xyz)
         return ener(self.tag, xyz[:, 0], xyz[:, 1], xyz[:, 2])
@@ -258,7 +264,8 @@ class Instance:
     def stats(self) -> dict:
         a = (ctypes.c_longlong * 16)()
         lib().agbnp3_stats(self.tag, a, 16)
-        return dict(near_pairs=a[0], kept=[a[1], a[2], a[3], a[4]], water_sites=a[6], error=a[7], launches=a[8])
+        return dict(near_pairs=a[0], kept=[a[1], a[2], a[3], a[4]], water_sites=a[6], error=a[7], launches=a[8],
+                    near_builds=a[9])
 
     def debug_fetch(self, what: int, count: int, dtype=np.int32):
         out = np.zeros(max(count, 1), dtype=dtype)
@@ -324,6 +331,9 @@ class Batch:
 
     def pair_order(self, mode: int = 1):
         _check(lib().agbnp3_batch_pair_order(self.btag, int(mode)), "agbnp3_batch_pair_order")
+
+    def set_nblist_skin(self, skin: float):
+        _check(lib().agbnp3_batch_set_nblist_skin(self.btag, float(skin)), "agbnp3_batch_set_nblist_skin")
 
     def set_coords(self, xyz):
         xyz = np.asarray(xyz, dtype=np.float64)

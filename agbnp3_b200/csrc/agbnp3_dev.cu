@@ -112,6 +112,14 @@ struct View {
      are a compact cluster (identity until the first evaluation sets it) */
   const int *slot_atom, *atom_slot;
   int *slot_type; /* radius type by slot */
+  /* Verlet-skin reuse of the near list (skin > 0): candidates j > g within
+     the near-list cutoff plus the skin, grouped by atom (CSR cand_off /
+     cand_cnt), the positions they were built from, and per candidate the
+     exact near-list flag and its exclusive scan */
+  float skin;
+  int cap_cand;
+  int *cand_j, *cand_own, *cand_flag, *cand_scan, *cand_off, *cand_cnt;
+  f4 *pos_ref;
   int *nl_c27, *nl_o27; /* near-list counts / offsets per (atom, neighbour cell) */
   int *nl_tmp, *nl_own; /* unsorted entries and their atom */
   int *ws_c27, *ws_o27, *ws_cand; /* water-site candidates per (site, cell) */
@@ -133,8 +141,12 @@ struct View {
 };
 
 enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m */, DC_C0 = DC_L0 + 8 /* scratch */,
-       DC_N27 = DC_C0 + 2, DC_W27, DC_WSC };
-#define DC_SIZE (DC_C0 + 8)
+       DC_N27 = DC_C0 + 2, DC_W27, DC_WSC,
+       /* Verlet skin: rebuild flag of this evaluation, candidate scan length
+          (27 N when rebuilding, else 0), that scan's total, the live
+          candidates of the last build, builds so far */
+       DC_REBUILD = DC_C0 + 8, DC_CLEN, DC_CTOT, DC_NCAND, DC_NBUILD };
+#define DC_SIZE (DC_C0 + 13)
 
 /* record fields of a kept overlap, stored contiguously per record (12
    slots, three 4-wide vectors) */
@@ -415,6 +427,137 @@ __global__ void k_nl_offsets(View v) {
     int o = v.nl_o27[27 * g], e = (g + 1 < v.natoms) ? v.nl_o27[27 * (g + 1)] : v.dc[DC_NL];
     v.nl_off[g] = o;
     v.nl_count[g] = e - o;
+  }
+}
+
+/* ---- Verlet skin ------------------------------------------------------ */
+/* The near list of an evaluation is exactly the cell-grid one: candidates
+   are the pairs within 1.6 (ri + rj) + skin when they were searched, and
+   while no heavy atom has moved skin/2 from those positions every pair now
+   within 1.6 (ri + rj) is among them; the reference's float test is
+   applied to the candidates at the current positions. */
+
+/* any heavy atom at skin/2 or more from its build position (or a build
+   forced by unset positions) sets the rebuild flag */
+__global__ void k_skin_check(View v) {
+  const float lim = 0.5f * v.skin * 0.9999f;
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int I = v.inst_of[g];
+    if (g >= v.inst_begin[I] + v.inst_nheavy[I]) continue;
+    f4 p = v.pos[g], q = v.pos_ref[g];
+    float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+    if (!(dx * dx + dy * dy + dz * dz < lim * lim)) v.dc[DC_REBUILD] = 1;
+  }
+}
+
+__global__ void k_skin_len(View v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int rb = v.dc[DC_REBUILD];
+    v.dc[DC_CLEN] = rb ? 27 * v.natoms : 0;
+    if (rb) v.dc[DC_NBUILD] += 1;
+  }
+}
+
+__device__ __forceinline__ bool cand_test(const f4 &a, const f4 &b, float skin) {
+  float dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
+  float u = 1.6f * (a.w + b.w) + skin + 1e-3f;
+  return dx * dx + dy * dy + dz * dz < u * u;
+}
+
+/* one thread per (heavy atom, neighbour cell), only when rebuilding */
+__global__ void k_cand_count27(View v) {
+  if (!v.dc[DC_REBUILD]) return;
+  AGB_GRID_STRIDE(q, 27LL * v.natoms) {
+    int g = (int)(q / 27), c = (int)(q % 27);
+    int I = v.inst_of[g];
+    int cnt = 0;
+    if (g < v.inst_begin[I] + v.inst_nheavy[I]) {
+      f4 a = v.pos[g];
+      for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
+               v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j, const f4 &b) {
+                 if (j > g && cand_test(a, b, v.skin)) cnt++;
+               });
+    }
+    v.nl_c27[q] = cnt;
+  }
+}
+
+__global__ void k_cand_emit27(View v) {
+  if (!v.dc[DC_REBUILD]) return;
+  AGB_GRID_STRIDE(q, 27LL * v.natoms) {
+    int n = v.nl_c27[q];
+    if (n == 0) continue;
+    int o = v.nl_o27[q];
+    if (o + n > v.cap_cand) {
+      set_err(v, AGB_ERR_CAND_CAP);
+      continue;
+    }
+    int g = (int)(q / 27), c = (int)(q % 27);
+    int I = v.inst_of[g];
+    f4 a = v.pos[g];
+    int m = 0;
+    for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
+             v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j, const f4 &b) {
+               if (j > g && cand_test(a, b, v.skin) && m < n) {
+                 v.cand_j[o + m] = j;
+                 v.cand_own[o + m] = g;
+                 m++;
+               }
+             });
+  }
+}
+
+/* per-atom candidate CSR and the build positions, only when rebuilding */
+__global__ void k_cand_offsets(View v) {
+  if (!v.dc[DC_REBUILD]) return;
+  const int tot = v.dc[DC_CTOT];
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int o = v.nl_o27[27 * g], e = (g + 1 < v.natoms) ? v.nl_o27[27 * (g + 1)] : tot;
+    v.cand_off[g] = o;
+    v.cand_cnt[g] = e - o;
+    v.pos_ref[g] = v.pos[g];
+    /* an overflowing build leaves no candidates (the evaluation is redone
+       with larger buffers) */
+    if (g == 0) v.dc[DC_NCAND] = tot <= v.cap_cand ? tot : 0;
+  }
+}
+
+/* the reference's test on every candidate at the current positions */
+__global__ void k_cand_flag(View v) {
+  int n = min(v.dc[DC_NCAND], v.cap_cand);
+  AGB_GRID_STRIDE(e, n) {
+    float d2;
+    v.cand_flag[e] = near_test(v.pos[v.cand_own[e]], v.pos[v.cand_j[e]], d2) ? 1 : 0;
+  }
+}
+
+__global__ void k_cand_nl_emit(View v) {
+  int n = min(v.dc[DC_NCAND], v.cap_cand);
+  AGB_GRID_STRIDE(e, n) {
+    if (!v.cand_flag[e]) continue;
+    int o = v.cand_scan[e];
+    if (o >= v.cap_nl) {
+      set_err(v, AGB_ERR_NL_CAP);
+      continue;
+    }
+    int g = v.cand_own[e], j = v.cand_j[e];
+    float d2;
+    near_test(v.pos[g], v.pos[j], d2);
+    v.nl_tmp[o] = j;
+    v.nl_d2[o] = d2;
+    v.nl_own[o] = g;
+  }
+}
+
+/* per-atom CSR of the filtered list: the scan at the atom's first and
+   past-last candidate */
+__global__ void k_cand_nl_offsets(View v) {
+  const int n = min(v.dc[DC_NCAND], v.cap_cand), tot = v.dc[DC_NL];
+  AGB_GRID_STRIDE(g, v.natoms) {
+    int a = v.cand_off[g], b = a + v.cand_cnt[g];
+    int sa = a < n ? v.cand_scan[a] : tot, sb = b < n ? v.cand_scan[b] : tot;
+    v.nl_off[g] = sa;
+    v.nl_count[g] = sb - sa;
   }
 }
 
@@ -2079,7 +2222,8 @@ struct agb_dev {
   void *allocs[128];
   int nallocs;
   /* tree capacity (owned separately, regrown on overflow) */
-  int cap_nl, cap[AGB_MAX_ORDER + 1], cap_wsc;
+  int cap_nl, cap[AGB_MAX_ORDER + 1], cap_wsc, cap_cand;
+  float *h_inst_cell; /* each instance's cell edge without a skin */
   int *scan_scratch;
   int scan_cap;
   double *esum, *ehb_inst, *o_energy;
@@ -2156,6 +2300,13 @@ static int tree_free(agb_dev *s) {
   s->v.nl_list = NULL;
   s->v.nl_d2 = NULL;
   s->scan_scratch = NULL;
+  int **cand[] = {&s->v.cand_j, &s->v.cand_own, &s->v.cand_flag, &s->v.cand_scan, &s->v.cand_off, &s->v.cand_cnt};
+  for (int k = 0; k < 6; k++) {
+    if (*cand[k]) cudaFree(*cand[k]);
+    *cand[k] = NULL;
+  }
+  if (s->v.pos_ref) cudaFree(s->v.pos_ref);
+  s->v.pos_ref = NULL;
   return 0;
 }
 
@@ -2189,6 +2340,23 @@ static int tree_alloc(agb_dev *s) {
   if (s->v.sf_nbuckets > s->scan_cap) s->scan_cap = s->v.sf_nbuckets;
   if (27 * s->natoms > s->scan_cap) s->scan_cap = 27 * s->natoms;
   if (27 * s->nws > s->scan_cap) s->scan_cap = 27 * s->nws;
+  s->v.cap_cand = 0;
+  if (s->v.skin > 0.0f) {
+    /* skin candidates; unset build positions force a search at the next
+       evaluation */
+    const size_t cc = (size_t)s->cap_cand, n = (size_t)s->natoms;
+    CK(cudaMalloc((void **)&s->v.cand_j, sizeof(int) * cc));
+    CK(cudaMalloc((void **)&s->v.cand_own, sizeof(int) * cc));
+    CK(cudaMalloc((void **)&s->v.cand_flag, sizeof(int) * cc));
+    CK(cudaMalloc((void **)&s->v.cand_scan, sizeof(int) * cc));
+    CK(cudaMalloc((void **)&s->v.cand_off, sizeof(int) * n));
+    CK(cudaMalloc((void **)&s->v.cand_cnt, sizeof(int) * n));
+    CK(cudaMalloc((void **)&s->v.pos_ref, sizeof(f4) * n));
+    CK(cudaMemsetAsync(s->v.pos_ref, 0x7f, sizeof(f4) * n, s->st));
+    CK(cudaMemsetAsync(s->v.dc + DC_NCAND, 0, sizeof(int), s->st));
+    s->v.cap_cand = s->cap_cand;
+    if (s->cap_cand > s->scan_cap) s->scan_cap = s->cap_cand;
+  }
   CK(cudaMalloc((void **)&s->scan_scratch, sizeof(int) * ((size_t)s->scan_cap / 1024 + 64)));
   s->v.cap_nl = s->cap_nl;
   return 0;
@@ -2352,6 +2520,8 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   UP(inst_of, inst_of, N, int);
   UP(inst_df, d->inst_df, NI, double);
   UP(inst_cell, d->inst_cell, NI, float);
+  s->h_inst_cell = (float *)malloc(sizeof(float) * NI);
+  memcpy(s->h_inst_cell, d->inst_cell, sizeof(float) * NI);
   UP(bucket_begin, bucket_begin, NI + 1, int);
   UP(bucket_mask, bucket_mask, NI, int);
   UP(ext_of, d->ext_of, N, int);
@@ -2581,6 +2751,7 @@ extern "C" void agb_dev_destroy(agb_dev *s) {
   free(s->h_ws_begin);
   free(s->h_inst_nheavy);
   free(s->h_ext_of);
+  free(s->h_inst_cell);
   free(s);
 }
 
@@ -2690,6 +2861,31 @@ static int order_pair_slots(agb_dev *s) {
   return 0;
 }
 
+extern "C" int agb_dev_set_skin(agb_dev *s, double skin) {
+  CK(cudaSetDevice(s->device));
+  if (!(skin >= 0.0 && skin <= 10.0)) FAIL("near-list skin %g outside [0, 10] A", skin);
+  CK(cudaStreamSynchronize(s->st));
+  if (s->graph_ok) {
+    cudaGraphExecDestroy(s->gexec);
+    s->graph_ok = 0;
+  }
+  tree_free(s);
+  s->v.skin = (float)skin;
+  if (skin > 0.0 && s->cap_cand == 0) {
+    /* the shell of width skin around the ~5.5 A cutoff adds candidates */
+    double f = 1.0 + skin / 5.0;
+    s->cap_cand = (int)(f * f * f * s->cap_nl) + 4096;
+  }
+  /* the cell grid must cover the candidate cutoff */
+  float *cell = (float *)malloc(sizeof(float) * s->ninst);
+  if (!cell) FAIL("out of host memory");
+  for (int I = 0; I < s->ninst; I++) cell[I] = s->h_inst_cell[I] + (float)skin;
+  int rc = upload((void *)s->v.inst_cell, cell, sizeof(float) * s->ninst);
+  free(cell);
+  if (rc) return -1;
+  return tree_alloc(s);
+}
+
 /* mode 1: order the pair slots along a Hilbert curve from the coordinates
    of the next evaluation (again on each call); mode 0: the identity */
 extern "C" int agb_dev_set_pair_order(agb_dev *s, int mode) {
@@ -2780,12 +2976,30 @@ static void launch_all(agb_dev *s) {
   AGB_LAUNCH(k_cell_count, nblocks(N), BLK, st, v);
   agb_scan_excl(v.bucket_count, v.bucket_start, v.dc + DC_NB, v.dc + DC_C0 + 7, v.nbuckets, s->scan_scratch, st);
   AGB_LAUNCH(k_cell_fill, nblocks(N), BLK, st, v);
-  AGB_LAUNCH(k_nl_count27, nblocks(27LL * N), BLK, st, v);
-  agb_scan_excl(v.nl_c27, v.nl_o27, v.dc + DC_N27, v.dc + DC_NL, 27 * N, s->scan_scratch, st);
-  AGB_LAUNCH(k_nl_emit27, nblocks(27LL * N), BLK, st, v);
-  AGB_LAUNCH(k_nl_offsets, nblocks(N), BLK, st, v);
+  if (v.skin > 0.0f) {
+    /* candidates searched only when an atom has moved skin/2 (the search
+       kernels return at once otherwise), filtered at every evaluation */
+    cudaMemsetAsync(v.dc + DC_REBUILD, 0, sizeof(int), st);
+    AGB_LAUNCH(k_skin_check, nblocks(N), BLK, st, v);
+    AGB_LAUNCH(k_skin_len, 1, 32, st, v);
+    AGB_LAUNCH(k_cand_count27, nblocks(27LL * N), BLK, st, v);
+    agb_scan_excl(v.nl_c27, v.nl_o27, v.dc + DC_CLEN, v.dc + DC_CTOT, 27 * N, s->scan_scratch, st);
+    AGB_LAUNCH(k_cand_emit27, nblocks(27LL * N), BLK, st, v);
+    AGB_LAUNCH(k_cand_offsets, nblocks(N), BLK, st, v);
+    AGB_LAUNCH(k_cand_flag, nblocks(s->cap_cand), BLK, st, v);
+    agb_scan_excl(v.cand_flag, v.cand_scan, v.dc + DC_NCAND, v.dc + DC_NL, s->cap_cand, s->scan_scratch, st);
+    AGB_LAUNCH(k_cand_nl_emit, nblocks(s->cap_cand), BLK, st, v);
+    AGB_LAUNCH(k_cand_nl_offsets, nblocks(N), BLK, st, v);
+    nl += 8 + 6;
+  } else {
+    AGB_LAUNCH(k_nl_count27, nblocks(27LL * N), BLK, st, v);
+    agb_scan_excl(v.nl_c27, v.nl_o27, v.dc + DC_N27, v.dc + DC_NL, 27 * N, s->scan_scratch, st);
+    AGB_LAUNCH(k_nl_emit27, nblocks(27LL * N), BLK, st, v);
+    AGB_LAUNCH(k_nl_offsets, nblocks(N), BLK, st, v);
+    nl += 3 + 3;
+  }
   AGB_LAUNCH(k_nl_rank, nblocks(s->cap_nl), BLK, st, v);
-  nl += 6 + 6;
+  nl += 6; /* cell grid (5) and ranking */
   stage_mark(s, 2);
   AGB_LAUNCH(k_l2_count<R>, nblocks(s->cap_nl), BLK, st, v);
   agb_scan_excl(v.lv_cnt[2], v.lv_off[2], v.dc + DC_NL, v.dc + DC_L0 + 2, s->cap_nl, s->scan_scratch, st);
@@ -2921,10 +3135,12 @@ extern "C" int agb_dev_evaluate(agb_dev *s) {
     s->last_stats[6] = s->nws;
     s->last_stats[7] = dc[DC_ERR];
     s->last_stats[8] = s->nlaunch;
+    s->last_stats[9] = dc[DC_NBUILD];
     int err = dc[DC_ERR];
-    if (err & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP | AGB_ERR_WS_CAP)) {
+    if (err & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP | AGB_ERR_WS_CAP | AGB_ERR_CAND_CAP)) {
       /* grow what overflowed and evaluate again */
       if (dc[DC_NL] > s->cap_nl) s->cap_nl = 2 * dc[DC_NL];
+      if ((err & AGB_ERR_CAND_CAP) && dc[DC_CTOT] > s->cap_cand) s->cap_cand = 2 * dc[DC_CTOT];
       if (dc[DC_WSC] > s->cap_wsc) s->cap_wsc = 2 * dc[DC_WSC];
       for (int m = 2; m <= AGB_MAX_ORDER; m++)
         if (dc[DC_L0 + m] > s->cap[m]) s->cap[m] = 2 * dc[DC_L0 + m];
@@ -3008,7 +3224,7 @@ extern "C" int agb_dev_stage_times(agb_dev *s, double *ms, int n) {
 
 extern "C" int agb_dev_stats(agb_dev *s, long long *out, int n) {
   for (int k = 0; k < n && k < 16; k++) out[k] = s->last_stats[k];
-  return 9;
+  return 10;
 }
 
 /* debug fetch ids */

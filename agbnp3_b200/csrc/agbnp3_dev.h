@@ -42,6 +42,7 @@ enum { AGB_PREC_FP64 = 0, AGB_PREC_MIXED = 1 };
 #define AGB_ERR_TREE_CAP 2
 #define AGB_ERR_WS_CAP 4
 #define AGB_ERR_NONFINITE 8
+#define AGB_ERR_CAND_CAP 16
 
 typedef struct {
   int ninst;
@@ -90,6 +91,11 @@ int agb_dev_evaluate(agb_dev *s);
 /* pair-stage slot order: 1 = along a Hilbert curve (set from the
    coordinates of the next evaluation), 0 = identity */
 int agb_dev_set_pair_order(agb_dev *s, int mode);
+/* Verlet skin (A) of the near list: 0 = searched on the cell grid at every
+   evaluation; > 0 = candidates within the cutoff plus skin, searched again
+   when a heavy atom has moved skin/2 since the last search, filtered
+   exactly at every evaluation */
+int agb_dev_set_skin(agb_dev *s, double skin);
 /* device -> host copies of the outputs of the last evaluation (any pointer
    may be NULL).  energies: [ninst][7] egb evdw ecorr_vdw ecav ecorr_cav ehb
    mol_volume.  Gradients are AoS [natoms][3], external order. */

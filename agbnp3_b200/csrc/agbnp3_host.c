@@ -738,6 +738,16 @@ int agbnp3_pair_order(int tag, int mode) {
   return AGBNP_OK;
 }
 
+int agbnp3_set_nblist_skin(int tag, double skin) {
+  inst_t *I = get_inst(tag, "agbnp3_set_nblist_skin()");
+  if (!I) return AGBNP_ERR;
+  if (agb_dev_set_skin(I->dev, skin) != 0) {
+    errprint("agbnp3_set_nblist_skin(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  return AGBNP_OK;
+}
+
 int agbnp3_get_mode(int tag, int *precision, int *compat) {
   inst_t *I = get_inst(tag, "agbnp3_get_mode()");
   if (!I) return AGBNP_ERR;
@@ -1012,6 +1022,16 @@ int agbnp3_batch_pair_order(int btag, int mode) {
   if (!B) return AGBNP_ERR;
   if (agb_dev_set_pair_order(B->dev, mode) != 0) {
     errprint("agbnp3_batch_pair_order(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  return AGBNP_OK;
+}
+
+int agbnp3_batch_set_nblist_skin(int btag, double skin) {
+  batch_t *B = get_batch(btag, "agbnp3_batch_set_nblist_skin()");
+  if (!B) return AGBNP_ERR;
+  if (agb_dev_set_skin(B->dev, skin) != 0) {
+    errprint("agbnp3_batch_set_nblist_skin(): %s", agb_dev_last_error());
     return AGBNP_ERR;
   }
   return AGBNP_OK;

@@ -39,6 +39,16 @@ int agbnp3_get_mode(int tag, int *precision, int *compat);
    summation order of the pair sums. */
 int agbnp3_pair_order(int tag, int mode);
 
+/* Verlet skin of the heavy-atom near list, in A (no counterpart in the
+   reference, which searches the list again on every call, agbnp3.c:1336).
+   skin = 0 (default): the list is searched on the cell grid at every
+   evaluation.  skin > 0: candidate pairs within 1.6 (ri + rj) + skin are
+   kept and searched again only when a heavy atom has moved skin/2 since
+   they were found; every evaluation applies the reference's float test to
+   the candidates, so the near list, and every result, is the same as
+   without a skin.  For MD callers whose atoms move little per step. */
+int agbnp3_set_nblist_skin(int tag, double skin);
+
 /* CUDA device used by instances created afterwards (default: $AGBNP3_DEVICE,
    else $LOCAL_RANK, else 0) */
 int agbnp3_set_device(int device);
@@ -77,7 +87,8 @@ const char *agbnp3_stage_name(int stage);
 
 /* counters of the last evaluation: [0] near-list pairs, [1..4] kept overlaps
    of orders 2..5, [5] unused, [6] water sites, [7] device error word,
-   [8] kernel launches per evaluation */
+   [8] kernel launches per evaluation, [9] near-list candidate searches so
+   far (with a Verlet skin) */
 int agbnp3_stats(int tag, long long *out, int n);
 
 /* internal arrays of the last evaluation, for parity tests (see
@@ -110,6 +121,7 @@ int agbnp3_batch_get_results(int btag, double *energies, double *sp, double *br,
 int agbnp3_batch_set_mode(int btag, int precision, int compat);
 /* agbnp3_pair_order for a batch (every member's atoms ordered separately) */
 int agbnp3_batch_pair_order(int btag, int mode);
+int agbnp3_batch_set_nblist_skin(int btag, double skin);
 /* agbnp3_ener_device for a batch: arrays span all members, concatenated
    in member order; energies [7 * members] */
 int agbnp3_batch_ener_device(int btag, const double *x, const double *y, const double *z, double *energies,
