@@ -67,6 +67,11 @@ def lib():
         L.agbnp3_pair_order.argtypes = [ctypes.c_int, ctypes.c_int]
         L.agbnp3_batch_pair_order.argtypes = [ctypes.c_int, ctypes.c_int]
         L.agbnp3_set_nblist_skin.argtypes = [ctypes.c_int, ctypes.c_double]
+        L.agbnp3_shard_unique_id.argtypes = [_vp, ctypes.c_int]
+        L.agbnp3_shard.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int]
+        L.agbnp3_shard_segment.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.agbnp3_shard_buffers.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int]
+        L.agbnp3_shard_buffers.restype = ctypes.c_longlong
         L.agbnp3_batch_set_nblist_skin.argtypes = [ctypes.c_int, ctypes.c_double]
         L.agbnp3_set_device.argtypes = [ctypes.c_int]
         L.agbnp3_set_coords.argtypes = [ctypes.c_int, _dp, _dp, _dp]
@@ -117,6 +122,16 @@ def _p(a, t=_dp):
 
 def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def shard_unique_id() -> bytes:
+    """NCCL unique id for a row-sharded instance (made on rank 0 and passed
+    to every rank, agbnp3_shard_unique_id)"""
+    buf = ctypes.create_string_buffer(512)
+    n = lib().agbnp3_shard_unique_id(ctypes.cast(buf, _vp), 512)
+    if n <= 0:
+        raise AGBNPError(f"agbnp3_shard_unique_id failed: {last_error()}")
+    return buf.raw[:n]
 
 
 def measure_peaks(device: int = 0) -> dict:
@@ -219,6 +234,35 @@ class Instance:
     def set_nblist_skin(self, skin: float):
         """Verlet skin (A) of the near list; 0 searches it at every evaluation"""
         _check(lib().agbnp3_set_nblist_skin(self.tag, float(skin)), "agbnp3_set_nblist_skin")
+
+    def shard(self, rank: int, nranks: int, uid: bytes | None = None):
+        """This instance as rank `rank` of `nranks` of a row-sharded
+        evaluation (agbnp3_shard); uid from shard_unique_id() on rank 0, or
+        None for segment-wise evaluation with caller-side sums."""
+        if uid is None:
+            _check(lib().agbnp3_shard(self.tag, int(rank), int(nranks), None, 0), "agbnp3_shard")
+        else:
+            buf = ctypes.create_string_buffer(bytes(uid), len(uid))
+            _check(lib().agbnp3_shard(self.tag, int(rank), int(nranks), ctypes.cast(buf, _vp), len(uid)),
+                   "agbnp3_shard")
+
+    def shard_segment(self, k: int):
+        _check(lib().agbnp3_shard_segment(self.tag, int(k)), "agbnp3_shard_segment")
+
+    def shard_sums(self, k: int) -> np.ndarray:
+        """partial sums of pair pass k on this rank, concatenated"""
+        n = lib().agbnp3_shard_buffers(self.tag, int(k), None, 0)
+        if n < 0:
+            raise AGBNPError(last_error())
+        out = np.empty(n)
+        if lib().agbnp3_shard_buffers(self.tag, int(k), _p(out), 0) != n:
+            raise AGBNPError(last_error())
+        return out
+
+    def set_shard_sums(self, k: int, sums: np.ndarray):
+        sums = np.ascontiguousarray(sums, dtype=np.float64)
+        if lib().agbnp3_shard_buffers(self.tag, int(k), _p(sums), 1) != sums.size:
+            raise AGBNPError(last_error())
 
     def ener(self, xyz=None) -> dict:
         xyz = self.system.coords() if xyz is None else np.asarray(xyz)

@@ -59,7 +59,7 @@ def build(force=False, verbose=False):
             log.append(_run(["gcc", "-O2", "-fPIC", "-std=c11", "-Wall", "-I", CSRC, "-I", INC,
                              "-I", "/usr/local/cuda/include", "-c", src, "-o", obj]))
     if force or _stale(LIB, objs):
-        log.append(_run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]))
+        log.append(_run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-ldl"]))
     gsrc = os.path.join(CSRC, "globule.c")
     if force or _stale(GLOBULE, [gsrc]):
         log.append(_run(["gcc", "-O2", "-shared", "-fPIC", "-o", GLOBULE, gsrc, "-lm"]))

@@ -38,6 +38,8 @@
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <dlfcn.h>
+#include <nccl.h>
 #include <float.h>
 #include <limits.h>
 #include <math.h>
@@ -2207,6 +2209,42 @@ static char g_err[512];
 
 extern "C" const char *agb_dev_last_error(void) { return g_err; }
 
+/* NCCL, loaded when a sharded instance is first set up (the process may
+   already hold the copy its framework loaded, which dlopen then returns) */
+static struct {
+  int loaded;
+  ncclResult_t (*GetUniqueId)(ncclUniqueId *);
+  ncclResult_t (*CommInitRank)(ncclComm_t *, int, ncclUniqueId, int);
+  ncclResult_t (*CommDestroy)(ncclComm_t);
+  ncclResult_t (*AllReduce)(const void *, void *, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t, cudaStream_t);
+  ncclResult_t (*GroupStart)(void);
+  ncclResult_t (*GroupEnd)(void);
+  const char *(*GetErrorString)(ncclResult_t);
+} g_nccl;
+
+static int nccl_load(void) {
+  if (g_nccl.loaded) return 0;
+  void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+  if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+  if (!h) FAIL("NCCL is not available: %s", dlerror());
+#define NCCL_SYM(f)                                              \
+  do {                                                           \
+    *(void **)&g_nccl.f = dlsym(h, "nccl" #f);                   \
+    if (!g_nccl.f) FAIL("NCCL has no symbol nccl%s", #f);        \
+  } while (0)
+  NCCL_SYM(GetUniqueId);
+  NCCL_SYM(CommInitRank);
+  NCCL_SYM(CommDestroy);
+  NCCL_SYM(AllReduce);
+  NCCL_SYM(GroupStart);
+  NCCL_SYM(GroupEnd);
+  NCCL_SYM(GetErrorString);
+#undef NCCL_SYM
+  g_nccl.loaded = 1;
+  return 0;
+}
+
+
 static const char *stage_names[AGB_NSTAGE] = {"prep",  "nblist", "volumes", "scaling", "invb",  "agb",
                                               "gbders", "ws",     "treeders", "final",  "reduce", "spare"};
 
@@ -2248,6 +2286,13 @@ struct agb_dev {
   int sfeat_ready; /* the feature kernel's shared-memory limit is set */
   int *h_inst_nheavy;
   int *h_ext_of;  /* external index of each internal atom */
+  /* row sharding of one instance over ranks (one GPU each): this rank's
+     share of the pair-stage items, and the communicator that sums the
+     pair stages' per-atom partial sums (NULL: emulated, see
+     agb_dev_shard_segment) */
+  int shard_rank, shard_n;
+  ncclComm_t comm;
+  int nccl_err;
   int pair_order; /* 1: pair slots along a Hilbert curve, 0: identity */
   int order_ok;   /* the slot order is set for the current mode */
 };
@@ -2431,15 +2476,27 @@ static int build_items(agb_dev *s, int nch, int jb) {
         }
     }
   }
+  if (s->shard_n > 1) {
+    /* this rank's share: every shard_n-th item of each list, so that every
+       pair is evaluated by exactly one rank and long and short j runs are
+       spread over the ranks */
+    int4 *L[3] = {it, ia, ig};
+    int *cnt[3] = {&nit, &na, &ng};
+    for (int k = 0; k < 3; k++) {
+      int m = 0;
+      for (int q = s->shard_rank; q < *cnt[k]; q += s->shard_n) L[k][m++] = L[k][q];
+      *cnt[k] = m;
+    }
+  }
   if (s->items) cudaFree(s->items);
   if (s->items_agb) cudaFree(s->items_agb);
   if (s->items_gbd) cudaFree(s->items_gbd);
   s->items = s->items_agb = s->items_gbd = NULL;
-  CK(cudaMalloc((void **)&s->items, sizeof(int4) * nit));
+  CK(cudaMalloc((void **)&s->items, sizeof(int4) * (nit + 1)));
   CK(cudaMalloc((void **)&s->items_agb, sizeof(int4) * (na + 1)));
   CK(cudaMalloc((void **)&s->items_gbd, sizeof(int4) * (ng + 1)));
-  CK(cudaMemcpy(s->items, it, sizeof(int4) * nit, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(s->items_agb, ia, sizeof(int4) * na, cudaMemcpyHostToDevice));
+  if (nit) CK(cudaMemcpy(s->items, it, sizeof(int4) * nit, cudaMemcpyHostToDevice));
+  if (na) CK(cudaMemcpy(s->items_agb, ia, sizeof(int4) * na, cudaMemcpyHostToDevice));
   if (ng) CK(cudaMemcpy(s->items_gbd, ig, sizeof(int4) * ng, cudaMemcpyHostToDevice));
   s->nitems = nit;
   s->n_agb = na;
@@ -2735,6 +2792,7 @@ extern "C" void agb_dev_destroy(agb_dev *s) {
   cudaSetDevice(s->device);
   cudaStreamSynchronize(s->st);
   if (s->graph_ok) cudaGraphExecDestroy(s->gexec);
+  if (s->comm) g_nccl.CommDestroy(s->comm);
   tree_free(s);
   for (int k = 0; k < s->nallocs; k++) cudaFree(s->allocs[k]);
   for (int k = 0; k <= AGB_NSTAGE; k++)
@@ -2959,12 +3017,45 @@ static void stage_mark(agb_dev *s, int k) {
 }
 
 /* the whole evaluation as a fixed launch sequence */
+/* the per-atom partial sums of pair stage k (0 descreening, 1 GB pair,
+   2 chain rule) that a row-sharded evaluation adds over the ranks before
+   the next stage reads them; returns how many arrays */
+static int shard_bufs(agb_dev *s, int k, double **ptr, size_t *cnt) {
+  const size_t N = (size_t)s->natoms;
+  View &v = s->v;
+  if (k == 0) {
+    ptr[0] = v.acc_beta, cnt[0] = N;
+    return 1;
+  }
+  if (k == 1) {
+    ptr[0] = v.dera, cnt[0] = N;
+    return 1;
+  }
+  /* the pair energy row of eatom, the constant-volume gradients and U, V;
+     nothing else has written these since they were zeroed */
+  ptr[0] = v.deru, cnt[0] = N;
+  ptr[1] = v.derv, cnt[1] = N;
+  ptr[2] = v.g_gb, cnt[2] = 3 * N;
+  ptr[3] = v.g_vw, cnt[3] = 3 * N;
+  ptr[4] = v.eatom + N, cnt[4] = N;
+  return 5;
+}
+
+static void shard_allreduce(agb_dev *s, int k, cudaStream_t st);
+
+/* the whole evaluation as a fixed launch sequence; seg >= 0 launches only
+   segment seg (0: up to the descreening sums, 1: Born radii and the GB pair
+   pass, 2: q2ab/abrw and the chain-rule pass, 3: the rest), between which a
+   row-sharded evaluation sums the pair stages' partial sums over the ranks */
 template <typename R>
-static void launch_all(agb_dev *s) {
+static void launch_all(agb_dev *s, int seg = -1) {
   View v = s->v;
   cudaStream_t st = s->st;
   int N = s->natoms;
   long long nl = 0;
+  /* the water-site stage on a side stream (captured whole evaluations) */
+  const bool side = !s->timing && s->nws > 0 && seg < 0;
+  if (seg < 0 || seg == 0) {
   stage_mark(s, 0);
   cudaMemsetAsync(v.bucket_count, 0, sizeof(int) * v.nbuckets, st);
   cudaMemsetAsync(v.bucket_cursor, 0, sizeof(int) * v.nbuckets, st);
@@ -3030,7 +3121,6 @@ static void launch_all(agb_dev *s) {
      scaling factors) and writes only its own outputs, the HB gradient and
      derh: in a captured evaluation it runs on a side stream beside the pair
      stages and joins before the tree-derivative pass */
-  const bool side = !s->timing && s->nws > 0;
   if (side) {
     cudaEventRecord(s->fork_ev, st);
     cudaStreamWaitEvent(s->st2, s->fork_ev, 0);
@@ -3038,18 +3128,26 @@ static void launch_all(agb_dev *s) {
     cudaEventRecord(s->join_ev, s->st2);
     nl += 4 + 3;
   }
-  int pgrid = s->nitems < 148 * 16 ? s->nitems : 148 * 16;
   int dgrid = s->nitems < 148 * 32 ? s->nitems : 148 * 32; /* 64-thread descreening blocks */
-  AGB_LAUNCH(k_descreen_t<R>, dgrid, ITILE / 2, st, v, s->items, s->nitems, s->nch);
+  AGB_LAUNCH(k_descreen_t<R>, dgrid > 0 ? dgrid : 1, ITILE / 2, st, v, s->items, s->nitems, s->nch);
+  nl += 1;
+  }
+  const int pgrid = s->nitems < 148 * 16 ? (s->nitems > 0 ? s->nitems : 1) : 148 * 16;
+  if (seg < 0) shard_allreduce(s, 0, st);
+  if (seg < 0 || seg == 1) {
   AGB_LAUNCH(k_born<R>, nblocks(N), BLK, st, v);
-  nl += 2;
+  nl += 1;
   stage_mark(s, 5);
   if (s->tiled_pairs)
     AGB_LAUNCH(k_agb_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
   else
     AGB_LAUNCH(k_agb_sym<R>, sym_grid(s->n_agb), 128, st, v, s->items_agb, s->n_agb);
+  nl += 1;
+  }
+  if (seg < 0) shard_allreduce(s, 1, st);
+  if (seg < 0 || seg == 2) {
   AGB_LAUNCH(k_agb_post<R>, nblocks(N), BLK, st, v);
-  nl += 2;
+  nl += 1;
   stage_mark(s, 6);
   if (s->tiled_pairs)
     AGB_LAUNCH(k_gbders_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
@@ -3057,8 +3155,12 @@ static void launch_all(agb_dev *s) {
     AGB_LAUNCH((k_gbders_sym<R, true>), sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
   else
     AGB_LAUNCH((k_gbders_sym<R, false>), sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
+  nl += 1;
+  }
+  if (seg < 0) shard_allreduce(s, 2, st);
+  if (seg < 0 || seg == 3) {
   AGB_LAUNCH(k_gbders_post, nblocks(N), BLK, st, v);
-  nl += 2;
+  nl += 1;
   stage_mark(s, 7);
   if (side) {
     cudaStreamWaitEvent(st, s->join_ev, 0);
@@ -3086,7 +3188,23 @@ static void launch_all(agb_dev *s) {
   AGB_LAUNCH(k_energies, 1, 128, st, s->esum, s->ehb_inst, s->ninst, s->o_energy, v.dc);
   nl += 4;
   stage_mark(s, 10);
-  s->nlaunch = nl;
+  }
+  if (seg < 0) s->nlaunch = nl;
+}
+
+/* in-place sums over the ranks of stage k's partial sums, one NCCL group
+   on the instance stream (captured with the rest of the evaluation) */
+static void shard_allreduce(agb_dev *s, int k, cudaStream_t st) {
+  if (!s->comm) return;
+  double *p[5];
+  size_t n[5];
+  int m = shard_bufs(s, k, p, n);
+  ncclResult_t r = g_nccl.GroupStart();
+  for (int q = 0; q < m && r == ncclSuccess; q++)
+    r = g_nccl.AllReduce(p[q], p[q], n[q], ncclFloat64, ncclSum, s->comm, st);
+  ncclResult_t r2 = g_nccl.GroupEnd();
+  if (r == ncclSuccess) r = r2;
+  if (r != ncclSuccess && !s->nccl_err) s->nccl_err = (int)r;
 }
 
 static int run_once(agb_dev *s) {
@@ -3127,6 +3245,11 @@ extern "C" int agb_dev_evaluate(agb_dev *s) {
      size is only known once the level below fits) */
   for (int attempt = 0; attempt < 16; attempt++) {
     if (run_once(s)) return -1;
+    if (s->nccl_err) {
+      int e = s->nccl_err;
+      s->nccl_err = 0;
+      FAIL("NCCL all-reduce of the sharded pair sums: %s", g_nccl.GetErrorString((ncclResult_t)e));
+    }
     int dc[DC_SIZE];
     CK(cudaMemcpyAsync(dc, s->v.dc, sizeof(dc), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -3156,6 +3279,95 @@ extern "C" int agb_dev_evaluate(agb_dev *s) {
     return 0;
   }
   FAIL("overlap buffers did not converge after regrowing");
+}
+
+extern "C" int agb_dev_shard_unique_id(void *id, int nbytes) {
+  if (nbytes < (int)sizeof(ncclUniqueId)) FAIL("unique id buffer of %d bytes, need %d", nbytes, (int)sizeof(ncclUniqueId));
+  if (nccl_load()) return -1;
+  ncclUniqueId u;
+  ncclResult_t r = g_nccl.GetUniqueId(&u);
+  if (r != ncclSuccess) FAIL("ncclGetUniqueId: %s", g_nccl.GetErrorString(r));
+  memcpy(id, &u, sizeof(u));
+  return (int)sizeof(u);
+}
+
+/* this instance as rank `rank` of `nranks`: pair-stage items split over the
+   ranks; with `id` (the same ncclUniqueId on every rank) the partial sums
+   are added over the ranks by NCCL inside each evaluation, without it the
+   evaluation only runs segment by segment (agb_dev_shard_segment) and the
+   caller adds them.  nranks = 1 without id undoes the sharding. */
+extern "C" int agb_dev_shard(agb_dev *s, int rank, int nranks, const void *id, int nbytes) {
+  CK(cudaSetDevice(s->device));
+  if (nranks < 1 || rank < 0 || rank >= nranks) FAIL("rank %d of %d", rank, nranks);
+  CK(cudaStreamSynchronize(s->st));
+  if (s->graph_ok) {
+    cudaGraphExecDestroy(s->gexec);
+    s->graph_ok = 0;
+  }
+  if (s->comm) {
+    g_nccl.CommDestroy(s->comm);
+    s->comm = NULL;
+  }
+  if (id) {
+    if (nbytes < (int)sizeof(ncclUniqueId)) FAIL("unique id of %d bytes, need %d", nbytes, (int)sizeof(ncclUniqueId));
+    if (nccl_load()) return -1;
+    ncclUniqueId u;
+    memcpy(&u, id, sizeof(u));
+    ncclComm_t c;
+    ncclResult_t r = g_nccl.CommInitRank(&c, nranks, u, rank);
+    if (r != ncclSuccess) FAIL("ncclCommInitRank(rank %d of %d): %s", rank, nranks, g_nccl.GetErrorString(r));
+    s->comm = c;
+  }
+  s->shard_rank = rank;
+  s->shard_n = nranks;
+  return build_items(s, s->nch, s->jb);
+}
+
+/* one segment of a sharded evaluation without a communicator, launched
+   directly and waited for: 0 .. 3, with the partial sums of pair stage k
+   exchanged through agb_dev_shard_buffers between segments k and k+1 */
+extern "C" int agb_dev_shard_segment(agb_dev *s, int k) {
+  CK(cudaSetDevice(s->device));
+  if (k < 0 || k > 3) FAIL("segment %d", k);
+  if (s->comm) FAIL("segments are for sharding without a communicator");
+  if (k == 0 && !s->order_ok && order_pair_slots(s)) return -1;
+  if (s->precision == AGB_PREC_FP64)
+    launch_all<double>(s, k);
+  else
+    launch_all<float>(s, k);
+  CK(cudaGetLastError());
+  int dc[DC_SIZE];
+  CK(cudaMemcpyAsync(dc, s->v.dc, sizeof(dc), cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  if (dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP | AGB_ERR_WS_CAP | AGB_ERR_CAND_CAP))
+    FAIL("buffer overflow in a segmented evaluation (error word %d): evaluate once unsharded first", dc[DC_ERR]);
+  if (k == 3) {
+    s->last_stats[0] = dc[DC_NL];
+    for (int m = 2; m <= AGB_MAX_ORDER; m++) s->last_stats[m - 1] = dc[DC_L0 + m];
+    s->last_stats[7] = dc[DC_ERR];
+    if (dc[DC_ERR] & AGB_ERR_NONFINITE) FAIL("non-finite energy");
+  }
+  return 0;
+}
+
+/* stage k's partial sums to (store 0) or from (store 1) host memory,
+   concatenated; returns the element count (host may be NULL to ask) */
+extern "C" long long agb_dev_shard_buffers(agb_dev *s, int k, double *host, int store) {
+  CK(cudaSetDevice(s->device));
+  if (k < 0 || k > 2) FAIL("stage %d", k);
+  double *p[5];
+  size_t n[5], tot = 0;
+  int m = shard_bufs(s, k, p, n);
+  for (int q = 0; q < m; q++) {
+    if (host) {
+      if (store)
+        CK(cudaMemcpy(p[q], host + tot, sizeof(double) * n[q], cudaMemcpyHostToDevice));
+      else
+        CK(cudaMemcpy(host + tot, p[q], sizeof(double) * n[q], cudaMemcpyDeviceToHost));
+    }
+    tot += n[q];
+  }
+  return (long long)tot;
 }
 
 extern "C" int agb_dev_download(agb_dev *s, double *energies, double *sp, double *br, double *surf_area,
@@ -3314,6 +3526,9 @@ extern "C" int agb_dev_autotune(agb_dev *s, int reps, const int *params_in, int 
     }
     return 0;
   }
+  /* timings differ between GPUs, and ranks whose work lists differ would
+     split the pairs inconsistently */
+  if (s->shard_n > 1) FAIL("a sharded instance is not tuned: pass the same explicit parameters on every rank");
   if (reps < 1) reps = 1;
   int timing = s->timing;
   s->timing = 1;

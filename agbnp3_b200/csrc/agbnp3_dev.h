@@ -96,6 +96,11 @@ int agb_dev_set_pair_order(agb_dev *s, int mode);
    when a heavy atom has moved skin/2 since the last search, filtered
    exactly at every evaluation */
 int agb_dev_set_skin(agb_dev *s, double skin);
+/* row sharding of one instance over ranks (one GPU each) */
+int agb_dev_shard_unique_id(void *id, int nbytes);
+int agb_dev_shard(agb_dev *s, int rank, int nranks, const void *id, int nbytes);
+int agb_dev_shard_segment(agb_dev *s, int k);
+long long agb_dev_shard_buffers(agb_dev *s, int k, double *host, int store);
 /* device -> host copies of the outputs of the last evaluation (any pointer
    may be NULL).  energies: [ninst][7] egb evdw ecorr_vdw ecav ecorr_cav ehb
    mol_volume.  Gradients are AoS [natoms][3], external order. */

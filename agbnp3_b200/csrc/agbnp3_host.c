@@ -748,6 +748,40 @@ int agbnp3_set_nblist_skin(int tag, double skin) {
   return AGBNP_OK;
 }
 
+int agbnp3_shard_unique_id(void *id, int nbytes) {
+  int n = agb_dev_shard_unique_id(id, nbytes);
+  if (n < 0) errprint("agbnp3_shard_unique_id(): %s", agb_dev_last_error());
+  return n < 0 ? AGBNP_ERR : n;
+}
+
+int agbnp3_shard(int tag, int rank, int nranks, const void *id, int nbytes) {
+  inst_t *I = get_inst(tag, "agbnp3_shard()");
+  if (!I) return AGBNP_ERR;
+  if (agb_dev_shard(I->dev, rank, nranks, id, nbytes) != 0) {
+    errprint("agbnp3_shard(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  return AGBNP_OK;
+}
+
+int agbnp3_shard_segment(int tag, int k) {
+  inst_t *I = get_inst(tag, "agbnp3_shard_segment()");
+  if (!I) return AGBNP_ERR;
+  if (agb_dev_shard_segment(I->dev, k) != 0) {
+    errprint("agbnp3_shard_segment(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  return AGBNP_OK;
+}
+
+long long agbnp3_shard_buffers(int tag, int k, double *host, int store) {
+  inst_t *I = get_inst(tag, "agbnp3_shard_buffers()");
+  if (!I) return AGBNP_ERR;
+  long long n = agb_dev_shard_buffers(I->dev, k, host, store);
+  if (n < 0) errprint("agbnp3_shard_buffers(): %s", agb_dev_last_error());
+  return n;
+}
+
 int agbnp3_get_mode(int tag, int *precision, int *compat) {
   inst_t *I = get_inst(tag, "agbnp3_get_mode()");
   if (!I) return AGBNP_ERR;

@@ -51,6 +51,9 @@ def parse():
                         "(per-term error of the chosen mode against the FP64 path); batch512: 512 instances of "
                         "300-5,000 atoms (log-uniform) with 0.2 A coordinate noise, one batched evaluation per step")
     p.add_argument("--ninst", type=int, default=512)
+    p.add_argument("--shard", action="store_true",
+                   help="strong scaling: ONE globule of --natoms atoms row-sharded over all ranks (NCCL all-reduce "
+                        "of the pair passes' partial sums inside each evaluation) instead of one conformation per rank")
     a = p.parse_args()
     if a.config == "globule100k":
         a.natoms = 100000
@@ -290,6 +293,64 @@ def batch_main(args, A, torch, rank, world, local):
         i.close()
 
 
+def shard_main(args, A, torch, rank, world, local):
+    """One instance row-sharded over all ranks (strong scaling): every rank
+    holds the same globule and evaluates its share of the pair passes; one
+    step = one whole evaluation, timed on every rank, max over ranks."""
+    from agbnp3_b200.shard import max_over_ranks, shard_instance
+    s = A.make_globule(args.natoms, args.seed)
+    inst = A.Instance(s, precision=A.PREC_MIXED, compat=True)
+    inst.ener()  # sizes the buffers and orders the pair slots
+    if world > 1:
+        shard_instance(inst)
+    else:
+        inst.shard(0, 1, A.shard_unique_id())
+    stream = torch.cuda.ExternalStream(inst.stream, device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    inst.set_coords(s.coords())
+    for _ in range(args.warmup):
+        inst.ener_resident()
+    times = []
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            inst.ener_resident()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    tot = max_over_ranks(sum(times), world, f"cuda:{local}")
+    R = inst.results()
+    # e2e: host coordinates in, all outputs out, every step, on every rank
+    e2e = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        inst.ener()
+        e2e.append(time.perf_counter() - t0)
+    e2e_tot = max_over_ranks(sum(e2e), world, f"cuda:{local}")
+    st = inst.stats()
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric_name(args.natoms) + ", one instance row-sharded", "value": args.steps / (tot / 1e3),
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tot / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 math / f64 accumulation", "data": "synthetic",
+            "config": {"workload": f"globule {args.natoms} atoms, seed {args.seed}, row-sharded over {world} ranks",
+                       "l2": "256 MB flush between timed steps"},
+            "e2e": {"value": args.steps / e2e_tot, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * args.natoms,
+                    "d2h_bytes_per_step": 15 * 8 * args.natoms + 56},
+            "gpu_launches": int(st["launches"]) * args.steps,
+            "energies": {k: R[k] for k in ("egb", "evdw", "ecav", "ehb")},
+            "clocks": clk.summary()}))
+    inst.close()
+
+
 # ----------------------------------------------------------------------------
 # engine arm
 # ----------------------------------------------------------------------------
@@ -308,8 +369,8 @@ def main():
     import agbnp3_b200 as A
     A.lib().agbnp3_set_device(local)
     A.initialize()
-    if args.config == "batch512":
-        batch_main(args, A, torch, rank, world, local)
+    if args.config == "batch512" or args.shard:
+        (shard_main if args.shard else batch_main)(args, A, torch, rank, world, local)
         A.terminate()
         if world > 1:
             torch.distributed.destroy_process_group()

@@ -49,6 +49,31 @@ int agbnp3_pair_order(int tag, int mode);
    without a skin.  For MD callers whose atoms move little per step. */
 int agbnp3_set_nblist_skin(int tag, double skin);
 
+/* Row sharding of ONE instance over several GPUs, one process (rank) per
+   GPU, each holding the whole instance (no counterpart in the reference,
+   which runs one instance on one host's OpenMP threads).  Each rank
+   evaluates every shard_n-th work item of the three pair passes
+   (descreening, GB pair, chain rule) and all other stages in full; the
+   pair passes' per-atom partial sums (descreening sums; A_i; U_i, V_i, the
+   pair gradients and the GB pair energies) are added over the ranks by
+   three NCCL all-reduces inside the evaluation, so every rank ends with
+   the complete outputs.  Every rank must evaluate the same coordinates,
+   collectively.
+   agbnp3_shard_unique_id: an ncclUniqueId (returns its size in bytes) that
+   rank 0 makes and passes to the others.  agbnp3_shard: this instance as
+   rank `rank` of `nranks` with that id; id = NULL splits the work without
+   a communicator, and evaluations then run only as the four segments of
+   agbnp3_shard_segment (0: up to the descreening sums, 1: Born radii and GB
+   pair pass, 2: the chain-rule pass, 3: the rest), the caller adding the
+   partial sums of pass k over the ranks in between with
+   agbnp3_shard_buffers (store 0: copy them out, concatenated; store 1: copy
+   the sums back; returns the element count, host may be NULL).
+   agbnp3_shard(tag, 0, 1, NULL, 0) undoes the sharding. */
+int agbnp3_shard_unique_id(void *id, int nbytes);
+int agbnp3_shard(int tag, int rank, int nranks, const void *id, int nbytes);
+int agbnp3_shard_segment(int tag, int k);
+long long agbnp3_shard_buffers(int tag, int k, double *host, int store);
+
 /* CUDA device used by instances created afterwards (default: $AGBNP3_DEVICE,
    else $LOCAL_RANK, else 0) */
 int agbnp3_set_device(int device);

@@ -44,3 +44,50 @@ def test_rank_zero_matches_single_gpu_run():
     assert rank_seed(11, 0) == 11
     a, b = make_globule(300, rank_seed(11, 0)), make_globule(300, 11)
     assert np.array_equal(a.x, b.x)
+
+
+class _FakeInstance:
+    """Records the agbnp3_shard call a rank would make."""
+
+    def __init__(self):
+        self.calls = []
+
+    def shard(self, rank, nranks, uid):
+        self.calls.append((rank, nranks, uid))
+
+
+def _shard_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from agbnp3_b200.shard import shard_instance
+        made = []
+
+        def make_id():  # only rank 0 may make the communicator's id
+            made.append(rank)
+            return os.urandom(128)
+
+        inst = _FakeInstance()
+        r, w = shard_instance(inst, make_id=make_id)
+        out[rank] = (r, w, inst.calls, made)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_shard_instance_id_exchange():
+    """Row sharding of one instance: rank 0 alone makes the NCCL unique id,
+    every rank joins with that same id, its own rank and the world size."""
+    world = 2
+    port = 30500 + os.getpid() % 1000
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_shard_worker, args=(world, port, out), nprocs=world, join=True)
+        res = [out[0], out[1]]
+    for rank, (r, w, calls, made) in enumerate(res):
+        assert (r, w) == (rank, world)
+        assert len(calls) == 1 and calls[0][:2] == (rank, world)
+        assert made == ([0] if rank == 0 else [])
+    assert res[0][2][0][2] == res[1][2][0][2] and len(res[0][2][0][2]) == 128
