@@ -29,6 +29,7 @@
    read from device memory; the sum goes to *total.  `cap` is the size of
    in/out and sizes the grid; scratch holds cap/1024+2 ints. */
 void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s);
+#define AGB_SCAN_LAUNCHES 2 /* kernels one agb_scan_excl launches */
 
 /* out[q*nseg + k] = sum of vals[q*stride + j] for j in [seg[k], seg[k+1]),
    for q < nq; one block per (q, k), fixed reduction order */

@@ -10,7 +10,7 @@
 #define SCAN_ITEMS 4 /* items per thread */
 #define SCAN_TILE (SCAN_BLOCK * SCAN_ITEMS)
 
-/* phases 1 and 3 run a fixed grid that loops over the live tiles, so a
+/* both phases run a fixed grid that loops over the live tiles, so a
    buffer sized for the worst case costs nothing beyond its live length */
 
 /* phase 1: tile sums */
@@ -36,47 +36,42 @@ __global__ void k_scan_tiles(const int *__restrict__ in, const int *__restrict__
   }
 }
 
-/* phase 2: exclusive scan of the tile sums in one block; writes the total */
-__global__ void k_scan_tile_sums(int *__restrict__ tile_sum, const int *__restrict__ n, int cap, int *__restrict__ total) {
-  __shared__ int sh[32];
-  int len = min(*n, cap);
-  int ntiles = (len + SCAN_TILE - 1) / SCAN_TILE;
-  int carry = 0;
-  for (int base = 0; base < ntiles; base += SCAN_BLOCK) {
-    int i = base + threadIdx.x;
-    int v = i < ntiles ? tile_sum[i] : 0;
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int x = v;
-    for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += t;
-    }
-    if (lane == 31) sh[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-      int w = sh[lane];
-      for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, w, o);
-        if (lane >= o) w += t;
-      }
-      sh[lane] = w;
-    }
-    __syncthreads();
-    int incl = x + (warp > 0 ? sh[warp - 1] : 0);
-    int chunk = sh[31];
-    if (i < ntiles) tile_sum[i] = carry + incl - v;
-    carry += chunk;
-    __syncthreads();
+/* sum over the block of one int per thread (sh: 32 ints of scratch,
+   free on entry and on return) */
+__device__ __forceinline__ int block_sum(int x, int *sh) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  if (lane == 0) sh[warp] = x;
+  __syncthreads();
+  int t = 0;
+  if (warp == 0) {
+    t = lane < SCAN_BLOCK / 32 ? sh[lane] : 0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) sh[0] = t;
   }
-  if (threadIdx.x == 0) *total = carry;
+  __syncthreads();
+  t = sh[0];
+  __syncthreads();
+  return t;
 }
 
-/* phase 3: scan inside each tile, offset by the tile's prefix */
+/* phase 2: scan inside each tile, offset by the sum of the tiles before it
+   (each block adds those tile sums itself: a few hundred ints); the block
+   of the last tile writes the total */
 __global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, const int *__restrict__ n, int cap,
-                             const int *__restrict__ tile_sum) {
+                             const int *__restrict__ tile_sum, int *__restrict__ total) {
   __shared__ int sh[32];
   const int len = min(*n, cap);
+  const long long ntiles = ((long long)len + SCAN_TILE - 1) / SCAN_TILE;
+  if (len <= 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *total = 0;
+    return;
+  }
   for (long long base = (long long)blockIdx.x * SCAN_TILE; base < len; base += (long long)gridDim.x * SCAN_TILE) {
+    const long long tile = base / SCAN_TILE;
+    int p = 0;
+    for (long long u = threadIdx.x; u < tile; u += SCAN_BLOCK) p += tile_sum[u];
+    const int prefix = block_sum(p, sh);
     int v[SCAN_ITEMS];
     int s = 0;
     for (int k = 0; k < SCAN_ITEMS; k++) {
@@ -101,12 +96,13 @@ __global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, 
       sh[lane] = w;
     }
     __syncthreads();
-    int run = tile_sum[base / SCAN_TILE] + x - s + (warp > 0 ? sh[warp - 1] : 0);
+    int run = prefix + x - s + (warp > 0 ? sh[warp - 1] : 0);
     for (int k = 0; k < SCAN_ITEMS; k++) {
       long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
       if (i < len) out[i] = run;
       run += v[k];
     }
+    if (tile == ntiles - 1 && threadIdx.x == SCAN_BLOCK - 1) *total = run;
     __syncthreads(); /* sh is reused by the next tile */
   }
 }
@@ -116,8 +112,7 @@ void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, i
   if (ntiles < 1) ntiles = 1;
   int grid = ntiles < 148 * 2 ? ntiles : 148 * 2; /* two 1024-thread blocks per SM */
   AGB_LAUNCH(k_scan_tiles, grid, SCAN_BLOCK, s, in, n, cap, scratch);
-  AGB_LAUNCH(k_scan_tile_sums, 1, SCAN_BLOCK, s, scratch, n, cap, total);
-  AGB_LAUNCH(k_scan_apply, grid, SCAN_BLOCK, s, in, out, n, cap, scratch);
+  AGB_LAUNCH(k_scan_apply, grid, SCAN_BLOCK, s, in, out, n, cap, scratch, total);
 }
 
 #define SEG_BLOCK 256
