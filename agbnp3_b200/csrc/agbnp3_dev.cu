@@ -966,7 +966,8 @@ __device__ __forceinline__ void chunk_range(int p0, int p1, int c, int nch, int 
 #define ITILE 128
 
 /* a staged partner: position and 1/(R h) in one vector record, the
-   descreening weight and radius type in another */
+   descreening weight and the offset of its radius type's column of tables
+   (type * AGB_NA records) in another */
 template <typename R>
 struct alignas(4 * sizeof(R)) Part4 {
   R x, y, z, rh;
@@ -976,6 +977,29 @@ struct alignas(2 * sizeof(R)) PartW {
   R w;
   int t;
 };
+
+/* one staged group of partners against a thread's two atoms; SELF: the
+   group may hold the atoms themselves (skipped) */
+template <typename R, bool SELF>
+__device__ __forceinline__ void desc_group(const Part4<R> *sp4, const PartW<R> *spw, int n, int j0, const int *g,
+                                           const R *xg, const R *yg, const R *zg,
+                                           const typename Tab<R>::T *const *rowp, R *part) {
+  for (int t = 0; t < n; t++) {
+    Part4<R> a = sp4[t];
+    PartW<R> b = spw[t];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      R dx = a.x - xg[u], dy = a.y - yg[u], dz = a.z - zg[u];
+      R xh = p_sqrt(dx * dx + dy * dy + dz * dz) * a.rh;
+      if (xh < R(AGB_NA - 1) && (!SELF || j0 + t != g[u])) {
+        int k = (int)xh;
+        R tt = xh - R(k);
+        typename Tab<R>::T c = Tab<R>::ld(rowp[u] + b.t + k);
+        part[u] += b.w * (c.x + tt * (c.y + tt * (c.z + tt * c.w)));
+      }
+    }
+  }
+}
 
 /* blocks of ITILE/2 threads, each thread two atoms of the ITILE-atom item */
 template <typename R>
@@ -993,6 +1017,7 @@ __global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__
     bool act[2];
     R xg[2], yg[2], zg[2];
     int row[2];
+    const typename Tab<R>::T *rowp[2];
     double acc[2] = {0.0, 0.0};
 #pragma unroll
     for (int u = 0; u < 2; u++) {
@@ -1002,6 +1027,7 @@ __global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__
       yg[u] = act[u] ? Y[g[u]] : R(0);
       zg[u] = act[u] ? Z[g[u]] : R(0);
       row[u] = act[u] ? v.slot_type[g[u]] * nt : 0;
+      rowp[u] = tab + (size_t)row[u] * AGB_NA;
     }
     int p0 = v.inst_begin[w.x], c0, c1;
     chunk_range(p0, p0 + v.inst_nheavy[w.x], w.w, nch, c0, c1);
@@ -1017,22 +1043,18 @@ __global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__
         sp4[t] = a;
         PartW<R> b;
         b.w = W[j0 + t];
-        b.t = v.slot_type[j0 + t];
+        b.t = v.slot_type[j0 + t] * AGB_NA;
         spw[t] = b;
       }
       AGB_SYNC();
       if (act[0]) {
         R part[2] = {R(0), R(0)};
-        for (int t = 0; t < n; t++) {
-          Part4<R> a = sp4[t];
-          PartW<R> b = spw[t];
-#pragma unroll
-          for (int u = 0; u < 2; u++) {
-            R dx = a.x - xg[u], dy = a.y - yg[u], dz = a.z - zg[u];
-            R xh = p_sqrt(dx * dx + dy * dy + dz * dz) * a.rh;
-            if (xh < R(AGB_NA - 1) && j0 + t != g[u]) part[u] += b.w * spline_z<R>(tab, row[u] + b.t, xh);
-          }
-        }
+        /* the item's own atoms are among the partners only when the staged
+           range overlaps the item (warp-uniform) */
+        if (j0 < w.z && j0 + n > w.y)
+          desc_group<R, true>(sp4, spw, n, j0, g, xg, yg, zg, rowp, part);
+        else
+          desc_group<R, false>(sp4, spw, n, j0, g, xg, yg, zg, rowp, part);
         acc[0] += (double)part[0];
         acc[1] += (double)part[1];
       }
