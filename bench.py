@@ -185,6 +185,13 @@ def reference_arm(args):
 PAIR_OPS = {"invb": (18, 1), "agb": (37, 2), "gbders_hh": (29 + 2 * 28, 1), "gbders_hx": (29 + 28, 1)}
 
 
+# DRAM bytes (read + write) per launch of the pair kernels, from the ncu
+# capture of the 25,000-atom globule (profiles/pair_kernels_globule25k_mixed.md;
+# ncu counters cannot be read inside the timed run); reported for that
+# workload only
+NCU_TRAFFIC_25K = {"k_gbders_sym": 2_728_960, "k_agb_sym": 2_025_216, "k_descreen_t": 1_075_200}
+
+
 def pair_roofline(natoms, nheavy, stage_ms, peaks):
     nx = natoms - nheavy
     work = {  # (flops, SFU ops) per launch
@@ -206,9 +213,13 @@ def pair_roofline(natoms, nheavy, stage_ms, peaks):
                                  "fp32_frac": tot_fl / (tot_ms * 1e-3) / 1e12 / peaks["fp32_tflops"]}
     dom = max(work, key=lambda k: stages[k]["ms"])
     d = stages[dom]
-    return {"kernel": {"gbders": "k_gbders_sym", "agb": "k_agb_sym", "invb": "k_descreen_t"}[dom],
+    kern = {"gbders": "k_gbders_sym", "agb": "k_agb_sym", "invb": "k_descreen_t"}[dom]
+    traffic = NCU_TRAFFIC_25K.get(kern) if natoms == 25000 else None
+    return {"kernel": kern,
             "stage": dom, "bound": "fp32", "achieved": d["tflops"], "peak": peaks["fp32_tflops"],
-            "unit": "TFLOP/s", "frac": d["fp32_frac"], "traffic": None,
+            "unit": "TFLOP/s", "frac": d["fp32_frac"], "traffic": traffic,
+            "traffic_note": "DRAM bytes per launch from the ncu capture in profiles/pair_kernels_globule25k_mixed.md "
+                            "(per-atom operands read once, per-atom sums written once)" if traffic else None,
             "peak_source": "measured in this run: FP32 FMA chains on every SM (agbnp3_measure_peaks)",
             "sfu_frac": d["sfu_frac"], "peaks": peaks, "stages": stages}
 
