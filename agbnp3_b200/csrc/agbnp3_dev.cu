@@ -1323,15 +1323,17 @@ __device__ __forceinline__ T rot1(T x) {
    each rotation step evaluates AGB_NI pairs with one set of shuffles.
    Interior j tiles (all valid, after the i block) skip the per-pair index
    tests. */
-/* i atoms per lane of the symmetric passes: four in FP32, two in FP64 (whose
-   wider registers would otherwise lower the occupancy) */
+/* i atoms per lane of the symmetric passes: in FP32 three (GB pair) and four
+   (chain rule), in FP64 two (whose wider registers would otherwise lower the
+   occupancy) */
 template <typename R>
 struct SymNI {
-  static constexpr int agb = sizeof(R) == 4 ? 4 : 2;
+  static constexpr int agb = sizeof(R) == 4 ? 3 : 2;
   static constexpr int gbd = sizeof(R) == 4 ? 4 : 2;
-  /* resident 128-thread blocks per SM asked of the GB pair pass in FP32
-     (80 registers: 6 blocks, 2.4 % faster than the 95-register build) */
-  static constexpr int agb_blocks = sizeof(R) == 4 ? 6 : 1;
+  /* resident 128-thread blocks per SM asked of the GB pair pass in FP32:
+     three i atoms per lane at 72 registers (7 blocks) measured faster than
+     four at 95 (5 blocks, 4 % slower) or 80 (6 blocks, 2 % slower) */
+  static constexpr int agb_blocks = sizeof(R) == 4 ? 7 : 1;
 };
 #define AGB_NI (SymNI<R>::agb)
 
