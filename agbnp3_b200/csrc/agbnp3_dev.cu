@@ -978,11 +978,7 @@ struct alignas(2 * sizeof(R)) PartW {
   int t;
 };
 
-/* atoms per thread of the descreening pass (its blocks: ITILE / DESC_U
-   threads) */
-#define DESC_U 2
-
-/* one staged group of partners against a thread's DESC_U atoms; SELF: the
+/* one staged group of partners against a thread's two atoms; SELF: the
    group may hold the atoms themselves (skipped) */
 template <typename R, bool SELF>
 __device__ __forceinline__ void desc_group(const Part4<R> *sp4, const PartW<R> *spw, int n, int j0, const int *g,
@@ -992,7 +988,7 @@ __device__ __forceinline__ void desc_group(const Part4<R> *sp4, const PartW<R> *
     Part4<R> a = sp4[t];
     PartW<R> b = spw[t];
 #pragma unroll
-    for (int u = 0; u < DESC_U; u++) {
+    for (int u = 0; u < 2; u++) {
       R dx = a.x - xg[u], dy = a.y - yg[u], dz = a.z - zg[u];
       R xh = p_sqrt(dx * dx + dy * dy + dz * dz) * a.rh;
       if (xh < R(AGB_NA - 1) && (!SELF || j0 + t != g[u])) {
@@ -1005,11 +1001,10 @@ __device__ __forceinline__ void desc_group(const Part4<R> *sp4, const PartW<R> *
   }
 }
 
-/* blocks of ITILE/DESC_U threads, each thread DESC_U atoms of the
-   ITILE-atom item */
+/* blocks of ITILE/2 threads, each thread two atoms of the ITILE-atom item */
 template <typename R>
-__global__ void __launch_bounds__(ITILE / DESC_U) k_descreen_t(View v, const int4 *__restrict__ items, int nitems,
-                                                               int nch) {
+__global__ void __launch_bounds__(ITILE / 2) k_descreen_t(View v, const int4 *__restrict__ items, int nitems,
+                                                          int nch) {
   AGB_SHARED Part4<R> sp4[ITILE];
   AGB_SHARED PartW<R> spw[ITILE];
   const R *X = pa<R>(v, PA_X), *Y = pa<R>(v, PA_Y), *Z = pa<R>(v, PA_Z);
@@ -1018,20 +1013,21 @@ __global__ void __launch_bounds__(ITILE / DESC_U) k_descreen_t(View v, const int
   const int nt = v.ntypes;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     int4 w = items[it];
-    int g[DESC_U];
-    bool act[DESC_U];
-    R xg[DESC_U], yg[DESC_U], zg[DESC_U];
-    const typename Tab<R>::T *rowp[DESC_U];
-    double acc[DESC_U];
+    int g[2];
+    bool act[2];
+    R xg[2], yg[2], zg[2];
+    int row[2];
+    const typename Tab<R>::T *rowp[2];
+    double acc[2] = {0.0, 0.0};
 #pragma unroll
-    for (int u = 0; u < DESC_U; u++) {
-      g[u] = w.y + threadIdx.x + u * (ITILE / DESC_U);
+    for (int u = 0; u < 2; u++) {
+      g[u] = w.y + threadIdx.x + u * (ITILE / 2);
       act[u] = g[u] < w.z;
       xg[u] = act[u] ? X[g[u]] : R(0);
       yg[u] = act[u] ? Y[g[u]] : R(0);
       zg[u] = act[u] ? Z[g[u]] : R(0);
-      rowp[u] = tab + (size_t)(act[u] ? v.slot_type[g[u]] * nt : 0) * AGB_NA;
-      acc[u] = 0.0;
+      row[u] = act[u] ? v.slot_type[g[u]] * nt : 0;
+      rowp[u] = tab + (size_t)row[u] * AGB_NA;
     }
     int p0 = v.inst_begin[w.x], c0, c1;
     chunk_range(p0, p0 + v.inst_nheavy[w.x], w.w, nch, c0, c1);
@@ -1052,21 +1048,19 @@ __global__ void __launch_bounds__(ITILE / DESC_U) k_descreen_t(View v, const int
       }
       AGB_SYNC();
       if (act[0]) {
-        R part[DESC_U];
-#pragma unroll
-        for (int u = 0; u < DESC_U; u++) part[u] = R(0);
+        R part[2] = {R(0), R(0)};
         /* the item's own atoms are among the partners only when the staged
            range overlaps the item (warp-uniform) */
         if (j0 < w.z && j0 + n > w.y)
           desc_group<R, true>(sp4, spw, n, j0, g, xg, yg, zg, rowp, part);
         else
           desc_group<R, false>(sp4, spw, n, j0, g, xg, yg, zg, rowp, part);
-#pragma unroll
-        for (int u = 0; u < DESC_U; u++) acc[u] += (double)part[u];
+        acc[0] += (double)part[0];
+        acc[1] += (double)part[1];
       }
     }
 #pragma unroll
-    for (int u = 0; u < DESC_U; u++)
+    for (int u = 0; u < 2; u++)
       if (act[u]) atomicAdd(&v.acc_beta[v.slot_atom[g[u]]], acc[u]);
   }
 }
@@ -3161,8 +3155,8 @@ static void launch_all(agb_dev *s, int seg = -1) {
     cudaEventRecord(s->join_ev, s->st2);
     nl += 4 + AGB_SCAN_LAUNCHES;
   }
-  int dgrid = s->nitems < 148 * 32 ? s->nitems : 148 * 32; /* small descreening blocks */
-  AGB_LAUNCH(k_descreen_t<R>, dgrid > 0 ? dgrid : 1, ITILE / DESC_U, st, v, s->items, s->nitems, s->nch);
+  int dgrid = s->nitems < 148 * 32 ? s->nitems : 148 * 32; /* 64-thread descreening blocks */
+  AGB_LAUNCH(k_descreen_t<R>, dgrid > 0 ? dgrid : 1, ITILE / 2, st, v, s->items, s->nitems, s->nch);
   nl += 1;
   }
   const int pgrid = s->nitems < 148 * 16 ? (s->nitems > 0 ? s->nitems : 1) : 148 * 16;
