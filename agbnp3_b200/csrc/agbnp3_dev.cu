@@ -92,6 +92,9 @@ struct View {
   f4 *cell_pos;  /* per bucket slot: the atom's position and radius */
   int2 *cell_id; /* per bucket slot: the atom and its packed cell */
   int *nl_count, *nl_off, *nl_list;
+  int slab_w;            /* near partners an atom's slab holds */
+  int *slab_j;           /* [natoms * slab_w] partners, unordered */
+  float *slab_d2;        /* [natoms * slab_w] their float d^2 */
   float *nl_d2;
   int cap_nl;
   int cap[AGB_MAX_ORDER + 1];
@@ -147,8 +150,9 @@ enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m
        /* Verlet skin: rebuild flag of this evaluation, candidate scan length
           (27 N when rebuilding, else 0), that scan's total, the live
           candidates of the last build, builds so far */
-       DC_REBUILD = DC_C0 + 8, DC_CLEN, DC_CTOT, DC_NCAND, DC_NBUILD };
-#define DC_SIZE (DC_C0 + 13)
+       DC_REBUILD = DC_C0 + 8, DC_CLEN, DC_CTOT, DC_NCAND, DC_NBUILD,
+       DC_SLABMAX /* near partners of the fullest overflowing slab */ };
+#define DC_SIZE (DC_C0 + 14)
 
 /* record fields of a kept overlap, stored contiguously per record (12
    slots, three 4-wide vectors) */
@@ -379,56 +383,59 @@ __device__ __forceinline__ void for_cell(const View &v, int I, int ax, int ay, i
   }
 }
 
-/* one thread per (heavy atom, neighbour cell): near partners j > i */
-__global__ void k_nl_count27(View v) {
+/* one thread per (heavy atom, neighbour cell): the atom's near partners
+   j > i go to its own slab of slab_w entries, in any order (the ranking
+   below fixes it), counted by an atomic per atom; an overflowing slab sets
+   the error word and the largest count needed */
+__global__ void k_nl_slab(View v) {
   AGB_GRID_STRIDE(q, 27LL * v.natoms) {
     int g = (int)(q / 27), c = (int)(q % 27);
     int I = v.inst_of[g];
-    int cnt = 0;
-    if (g < v.inst_begin[I] + v.inst_nheavy[I]) {
-      f4 a = v.pos[g];
-      for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
-               v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j, const f4 &b) {
-                 float d2;
-                 if (j > g && near_test(a, b, d2)) cnt++;
-               });
-    }
-    v.nl_c27[q] = cnt;
-  }
-}
-
-__global__ void k_nl_emit27(View v) {
-  AGB_GRID_STRIDE(q, 27LL * v.natoms) {
-    int n = v.nl_c27[q];
-    if (n == 0) continue;
-    int o = v.nl_o27[q];
-    if (o + n > v.cap_nl) {
-      set_err(v, AGB_ERR_NL_CAP);
-      continue;
-    }
-    int g = (int)(q / 27), c = (int)(q % 27);
-    int I = v.inst_of[g];
+    if (g >= v.inst_begin[I] + v.inst_nheavy[I]) continue;
     f4 a = v.pos[g];
-    int m = 0;
+    const size_t base = (size_t)g * v.slab_w;
     for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
              v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j, const f4 &b) {
                float d2;
-               if (j > g && near_test(a, b, d2) && m < n) {
-                 v.nl_tmp[o + m] = j;
-                 v.nl_d2[o + m] = d2;
-                 v.nl_own[o + m] = g;
-                 m++;
+               if (j > g && near_test(a, b, d2)) {
+                 int k = atomicAdd(&v.nl_count[g], 1);
+                 if (k < v.slab_w) {
+                   v.slab_j[base + k] = j;
+                   v.slab_d2[base + k] = d2;
+                 } else {
+                   set_err(v, AGB_ERR_NL_CAP);
+                   atomicMax(&v.dc[DC_SLABMAX], k + 1);
+                 }
                }
              });
   }
 }
 
-/* per-atom CSR of the near list */
-__global__ void k_nl_offsets(View v) {
-  AGB_GRID_STRIDE(g, v.natoms) {
-    int o = v.nl_o27[27 * g], e = (g + 1 < v.natoms) ? v.nl_o27[27 * (g + 1)] : v.dc[DC_NL];
-    v.nl_off[g] = o;
-    v.nl_count[g] = e - o;
+/* each atom's list in (float d^2, index) order (agbnp3.c:3766-3792,
+   4062-4066): one warp per atom, each slab entry placed at its rank */
+__global__ void k_nl_slab_rank(View v) {
+  if (v.dc[DC_ERR] & AGB_ERR_NL_CAP) return;
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long g = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < v.natoms; g += nw) {
+    const int m = v.nl_count[g], o = v.nl_off[g];
+    if (m == 0) continue;
+    if (o + m > v.cap_nl) {
+      if (lane == 0) set_err(v, AGB_ERR_NL_CAP);
+      continue;
+    }
+    const size_t base = (size_t)g * v.slab_w;
+    for (int k = lane; k < m; k += 32) {
+      const float d2 = v.slab_d2[base + k];
+      const int j = v.slab_j[base + k];
+      int rank = 0;
+      for (int b = 0; b < m; b++) {
+        float db = v.slab_d2[base + b];
+        rank += (db < d2) || (db == d2 && v.slab_j[base + b] < j);
+      }
+      v.nl_list[o + rank] = j;
+      v.nl_own[o + rank] = (int)g;
+    }
   }
 }
 
@@ -2287,7 +2294,7 @@ struct agb_dev {
   void *allocs[128];
   int nallocs;
   /* tree capacity (owned separately, regrown on overflow) */
-  int cap_nl, cap[AGB_MAX_ORDER + 1], cap_wsc, cap_cand;
+  int cap_nl, cap[AGB_MAX_ORDER + 1], cap_wsc, cap_cand, slab_w;
   float *h_inst_cell; /* each instance's cell edge without a skin */
   int *scan_scratch;
   int scan_cap;
@@ -2379,6 +2386,10 @@ static int tree_free(agb_dev *s) {
   }
   if (s->v.pos_ref) cudaFree(s->v.pos_ref);
   s->v.pos_ref = NULL;
+  if (s->v.slab_j) cudaFree(s->v.slab_j);
+  if (s->v.slab_d2) cudaFree(s->v.slab_d2);
+  s->v.slab_j = NULL;
+  s->v.slab_d2 = NULL;
   return 0;
 }
 
@@ -2391,6 +2402,12 @@ static int tree_alloc(agb_dev *s) {
   CK(cudaMalloc((void **)&s->v.nl_d2, sizeof(float) * (size_t)s->cap_nl));
   CK(cudaMalloc((void **)&s->v.nl_tmp, sizeof(int) * (size_t)s->cap_nl));
   CK(cudaMalloc((void **)&s->v.nl_own, sizeof(int) * (size_t)s->cap_nl));
+  s->v.slab_w = 0;
+  if (s->v.skin <= 0.0f) { /* the slabs of the per-evaluation search */
+    CK(cudaMalloc((void **)&s->v.slab_j, sizeof(int) * (size_t)s->natoms * s->slab_w));
+    CK(cudaMalloc((void **)&s->v.slab_d2, sizeof(float) * (size_t)s->natoms * s->slab_w));
+    s->v.slab_w = s->slab_w;
+  }
   int maxcap = s->natoms;
   for (int m = 2; m <= AGB_MAX_ORDER; m++) {
     CK(cudaMalloc((void **)&s->v.par[m], sizeof(int) * (size_t)m * s->cap[m]));
@@ -2798,6 +2815,7 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   s->cap[4] = 64 * nheavy_tot + 4096;
   s->cap[5] = 32 * nheavy_tot + 4096;
   s->cap_wsc = 64 * NW + 1024;
+  s->slab_w = 96; /* ~29 near partners j > i per heavy atom on average */
   /* AGBNP3_CAPACITY_SCALE (< 1) starts from smaller buffers, which
      exercises the overflow detection and regrowth of agb_dev_evaluate */
   const char *cs = getenv("AGBNP3_CAPACITY_SCALE");
@@ -2806,6 +2824,7 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     s->cap_nl = (int)(s->cap_nl * f) + 1;
     for (int m = 2; m <= AGB_MAX_ORDER; m++) s->cap[m] = (int)(s->cap[m] * f) + 1;
     s->cap_wsc = (int)(s->cap_wsc * f) + 1;
+    s->slab_w = (int)(s->slab_w * f) + 1;
   }
   if (tree_alloc(s)) return -1;
   for (int k = 0; k <= AGB_NSTAGE; k++) CK(cudaEventCreate(&s->ev[k]));
@@ -3108,16 +3127,17 @@ static void launch_all(agb_dev *s, int seg = -1) {
     agb_scan_excl(v.cand_flag, v.cand_scan, v.dc + DC_NCAND, v.dc + DC_NL, s->cap_cand, s->scan_scratch, st);
     AGB_LAUNCH(k_cand_nl_emit, nblocks(s->cap_cand), BLK, st, v);
     AGB_LAUNCH(k_cand_nl_offsets, nblocks(N), BLK, st, v);
-    nl += 8 + 2 * AGB_SCAN_LAUNCHES;
+    AGB_LAUNCH(k_nl_rank, nblocks(s->cap_nl), BLK, st, v);
+    nl += 9 + 2 * AGB_SCAN_LAUNCHES;
   } else {
-    AGB_LAUNCH(k_nl_count27, nblocks(27LL * N), BLK, st, v);
-    agb_scan_excl(v.nl_c27, v.nl_o27, v.dc + DC_N27, v.dc + DC_NL, 27 * N, s->scan_scratch, st);
-    AGB_LAUNCH(k_nl_emit27, nblocks(27LL * N), BLK, st, v);
-    AGB_LAUNCH(k_nl_offsets, nblocks(N), BLK, st, v);
-    nl += 3 + AGB_SCAN_LAUNCHES;
+    cudaMemsetAsync(v.nl_count, 0, sizeof(int) * N, st);
+    cudaMemsetAsync(v.dc + DC_SLABMAX, 0, sizeof(int), st);
+    AGB_LAUNCH(k_nl_slab, nblocks(27LL * N), BLK, st, v);
+    agb_scan_excl(v.nl_count, v.nl_off, v.dc + DC_N, v.dc + DC_NL, N, s->scan_scratch, st);
+    AGB_LAUNCH(k_nl_slab_rank, nblocks(32LL * N), BLK, st, v);
+    nl += 2 + AGB_SCAN_LAUNCHES;
   }
-  AGB_LAUNCH(k_nl_rank, nblocks(s->cap_nl), BLK, st, v);
-  nl += 3 + AGB_SCAN_LAUNCHES; /* cell grid and ranking */
+  nl += 2 + AGB_SCAN_LAUNCHES; /* cell grid */
   stage_mark(s, 2);
   AGB_LAUNCH(k_l2_count<R>, nblocks(s->cap_nl), BLK, st, v);
   agb_scan_excl(v.lv_cnt[2], v.lv_off[2], v.dc + DC_NL, v.dc + DC_L0 + 2, s->cap_nl, s->scan_scratch, st);
@@ -3290,6 +3310,7 @@ extern "C" int agb_dev_evaluate(agb_dev *s) {
     if (err & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP | AGB_ERR_WS_CAP | AGB_ERR_CAND_CAP)) {
       /* grow what overflowed and evaluate again */
       if (dc[DC_NL] > s->cap_nl) s->cap_nl = 2 * dc[DC_NL];
+      if (dc[DC_SLABMAX] > s->slab_w) s->slab_w = dc[DC_SLABMAX] + 32;
       if ((err & AGB_ERR_CAND_CAP) && dc[DC_CTOT] > s->cap_cand) s->cap_cand = 2 * dc[DC_CTOT];
       if (dc[DC_WSC] > s->cap_wsc) s->cap_wsc = 2 * dc[DC_WSC];
       for (int m = 2; m <= AGB_MAX_ORDER; m++)
