@@ -146,7 +146,7 @@ struct View {
 };
 
 enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m */, DC_C0 = DC_L0 + 8 /* scratch */,
-       DC_N27 = DC_C0 + 2, DC_W27, DC_WSC,
+       DC_W27 = DC_C0 + 2, DC_WSC,
        /* Verlet skin: rebuild flag of this evaluation, candidate scan length
           (27 N when rebuilding, else 0), that scan's total, the live
           candidates of the last build, builds so far */
@@ -2802,7 +2802,6 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   dc0[DC_N] = N;
   dc0[DC_NB] = nb;
   dc0[DC_NWS] = NW;
-  dc0[DC_N27] = 27 * N;
   dc0[DC_W27] = 27 * NW;
   if (upload(v.dc, dc0, sizeof(dc0))) return -1;
 
