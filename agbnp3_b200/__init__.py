@@ -73,6 +73,7 @@ def lib():
         L.agbnp3_shard_buffers.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int]
         L.agbnp3_shard_buffers.restype = ctypes.c_longlong
         L.agbnp3_batch_set_nblist_skin.argtypes = [ctypes.c_int, ctypes.c_double]
+        L.agbnp3_batch_stats.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
         L.agbnp3_set_device.argtypes = [ctypes.c_int]
         L.agbnp3_set_coords.argtypes = [ctypes.c_int, _dp, _dp, _dp]
         L.agbnp3_ener_resident.argtypes = [ctypes.c_int]
@@ -378,6 +379,12 @@ class Batch:
 
     def set_nblist_skin(self, skin: float):
         _check(lib().agbnp3_batch_set_nblist_skin(self.btag, float(skin)), "agbnp3_batch_set_nblist_skin")
+
+    def stats(self) -> dict:
+        a = (ctypes.c_longlong * 16)()
+        lib().agbnp3_batch_stats(self.btag, a, 16)
+        return dict(near_pairs=a[0], kept=[a[1], a[2], a[3], a[4]], water_sites=a[6], error=a[7], launches=a[8],
+                    near_builds=a[9])
 
     def set_coords(self, xyz):
         xyz = np.asarray(xyz, dtype=np.float64)

@@ -1061,6 +1061,11 @@ int agbnp3_batch_pair_order(int btag, int mode) {
   return AGBNP_OK;
 }
 
+int agbnp3_batch_stats(int btag, long long *out, int n) {
+  batch_t *B = get_batch(btag, "agbnp3_batch_stats()");
+  return B ? agb_dev_stats(B->dev, out, n) : AGBNP_ERR;
+}
+
 int agbnp3_batch_set_nblist_skin(int btag, double skin) {
   batch_t *B = get_batch(btag, "agbnp3_batch_set_nblist_skin()");
   if (!B) return AGBNP_ERR;

@@ -276,6 +276,7 @@ def batch_main(args, A, torch, rank, world, local):
         B.results()
         e2e.append(time.perf_counter() - t0)
     R = B.results()
+    launches = int(B.stats()["launches"])
     # accuracy of the batched mixed path against the FP64 path on 8 members
     acc = []
     for k in range(0, args.ninst, max(1, args.ninst // 8)):
@@ -298,6 +299,7 @@ def batch_main(args, A, torch, rank, world, local):
             "e2e": {"value": world * args.ninst * args.steps / sum(e2e), "unit": "evals/s",
                     "h2d_bytes_per_step": 3 * 8 * natoms, "d2h_bytes_per_step": 15 * 8 * natoms + 56 * args.ninst},
             "accuracy_vs_fp64": {"max_energy_rel_err": max(acc)},
+            "gpu_launches": launches * args.steps,
             "clocks": clk.summary()}))
     B.close()
     for i in insts:

@@ -147,6 +147,8 @@ int agbnp3_batch_set_mode(int btag, int precision, int compat);
 /* agbnp3_pair_order for a batch (every member's atoms ordered separately) */
 int agbnp3_batch_pair_order(int btag, int mode);
 int agbnp3_batch_set_nblist_skin(int btag, double skin);
+/* agbnp3_stats for a batch (counts over all members) */
+int agbnp3_batch_stats(int btag, long long *out, int n);
 /* agbnp3_ener_device for a batch: arrays span all members, concatenated
    in member order; energies [7 * members] */
 int agbnp3_batch_ener_device(int btag, const double *x, const double *y, const double *z, double *energies,
