@@ -104,3 +104,33 @@ def test_nccl_single_rank(engine):
     finally:
         inst.close()
         ref.close()
+
+
+def test_shard_with_skin_and_errors(engine):
+    """Sharding composes with the near-list skin; bad ranks and tuning a
+    sharded instance are refused."""
+    s, _ = load_golden("globule300_shuffled")
+    ref = A.Instance(s, precision=A.PREC_FP64)
+    ranks = [A.Instance(s, precision=A.PREC_FP64) for _ in range(2)]
+    try:
+        xyz = s.coords()
+        q = ref.ener(xyz)
+        for r, inst in enumerate(ranks):
+            inst.set_nblist_skin(1.0)
+            inst.ener(xyz)
+            inst.shard(r, 2)
+        for step in range(3):
+            for res in emulated_evaluation(ranks, xyz):
+                same_results(res, q)
+            xyz = s.with_coords(xyz + np.random.default_rng(10 + step).normal(0.0, 0.1, xyz.shape)).coords()
+            q = ref.ener(xyz)
+        with pytest.raises(A.AGBNPError):
+            ranks[0].shard(2, 2)
+        with pytest.raises(A.AGBNPError):
+            ranks[0].autotune()
+        with pytest.raises(A.AGBNPError):
+            ranks[0].shard_segment(4)
+    finally:
+        for inst in ranks:
+            inst.close()
+        ref.close()
