@@ -991,6 +991,7 @@ template <typename R, bool SELF>
 __device__ __forceinline__ void desc_group(const Part4<R> *sp4, const PartW<R> *spw, int n, int j0, const int *g,
                                            const R *xg, const R *yg, const R *zg,
                                            const typename Tab<R>::T *const *rowp, R *part) {
+#pragma unroll 4
   for (int t = 0; t < n; t++) {
     Part4<R> a = sp4[t];
     PartW<R> b = spw[t];
