@@ -1362,6 +1362,7 @@ struct AgbP {
 
 template <typename R, bool FULL>
 __device__ __forceinline__ void agb_tile(const AgbI<R> &I, AgbJ<R> &J, AgbP<R> &P, int lane, int j0, int a1) {
+  #pragma unroll 2
   for (int r = 0; r < 32; r++) {
     if (r > 0) {
       J.x = rot1(J.x); J.y = rot1(J.y); J.z = rot1(J.z);
