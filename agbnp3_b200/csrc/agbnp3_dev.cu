@@ -99,6 +99,8 @@ struct View {
   int cap_nl;
   int cap[AGB_MAX_ORDER + 1];
   int *lv_cnt[AGB_MAX_ORDER + 1], *lv_off[AGB_MAX_ORDER + 1];
+  unsigned long long *lv_mask[AGB_MAX_ORDER + 1]; /* kept siblings of each generating overlap */
+  int *lv_own[AGB_MAX_ORDER + 1];                 /* generating overlap of each record */
   int *par[AGB_MAX_ORDER + 1], *gend[AGB_MAX_ORDER + 1];
   void *rec[AGB_MAX_ORDER + 1];
   int *dc; /* device counters, DC_* */
@@ -746,7 +748,10 @@ __global__ void k_l2_emit(View v) {
 }
 
 /* order M >= 3: overlap a combines with the last atom of every later
-   overlap b of its group (same generating overlap one order down) */
+   overlap b of its group (same generating overlap one order down).  The
+   count pass also records which siblings were kept (bit b - a - 1 of a
+   64-bit mask; 0 for groups wider than 64, whose kept siblings the emit
+   pass finds again by search) */
 template <typename R, int M>
 __global__ void k_lm_count(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
@@ -754,66 +759,125 @@ __global__ void k_lm_count(View v) {
   const int cm = v.cap[M - 1];
   AGB_GRID_STRIDE(a, n) {
     int ge = v.gend[M - 1][a], cnt = 0;
+    unsigned long long mask = 0ull;
     const Ov<R> oa = rec_load<R>(v, M - 1, a);
     for (int b = a + 1; b < ge; b++) {
       int j = v.par[M - 1][(size_t)(M - 2) * cm + b];
       Ov<R> ov = ogauss<R>(oa.a, oa.p, oa.cx, oa.cy, oa.cz, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j),
                            pz<R>(v, j));
-      if (kept(ov.gvolp)) cnt++;
+      if (kept(ov.gvolp)) {
+        cnt++;
+        if (b - a <= 64) mask |= 1ull << (b - a - 1);
+      }
     }
     v.lv_cnt[M][a] = cnt;
+    v.lv_mask[M][a] = ge - a - 1 <= 64 ? mask : 0ull;
   }
 }
 
-/* the records of one thread share parents 0..M-2: their sums stay in
-   registers and go out with one atomic each at the end */
-template <typename R, int M>
-__global__ void k_lm_emit(View v) {
+/* the generating overlap of every order-M record (one thread per
+   generating overlap; a few records each) */
+template <int M>
+__global__ void k_lm_owner(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
   const int n = min(v.dc[DC_L0 + M - 1], v.cap[M - 1]);
-  const int cm = v.cap[M - 1], cn = v.cap[M];
   AGB_GRID_STRIDE(a, n) {
-    int q = v.lv_off[M][a], qend = q + v.lv_cnt[M][a];
-    if (q == qend) continue;
-    if (qend > cn) {
+    const int q = v.lv_off[M][a], c = v.lv_cnt[M][a];
+    if (q + c > v.cap[M]) {
       set_err(v, AGB_ERR_TREE_CAP);
       continue;
     }
-    int ge = v.gend[M - 1][a];
-    int par[M - 1];
-    double svol[M - 1], ssurf[M - 1];
+    for (int k = 0; k < c; k++) v.lv_own[M][q + k] = (int)a;
+  }
+}
+
+/* sum of a[0..NN) over the run of consecutive lanes holding this lane's
+   key; returns whether this lane ends its run */
+template <typename T, int NN>
+__device__ __forceinline__ bool seg_scan_n(T (&a)[NN], int key) {
+  const int lane = threadIdx.x & 31;
+  int kp = __shfl_up_sync(0xffffffffu, key, 1);
+  int kn = __shfl_down_sync(0xffffffffu, key, 1);
+  unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || kp != key);
+  int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+  const int span = __reduce_max_sync(0xffffffffu, lane - start);
+  for (int o = 1; o <= span; o <<= 1) {
+    bool take = lane - o >= start;
 #pragma unroll
-    for (int k = 0; k < M - 1; k++) {
-      par[k] = v.par[M - 1][(size_t)k * cm + a];
-      svol[k] = ssurf[k] = 0.0;
+    for (int c = 0; c < NN; c++) {
+      T t = __shfl_up_sync(0xffffffffu, a[c], o);
+      if (take) a[c] += t;
     }
-    const Ov<R> oa = rec_load<R>(v, M - 1, a);
-    for (int b = a + 1; b < ge; b++) {
-      int j = v.par[M - 1][(size_t)(M - 2) * cm + b];
-      Ov<R> ov = ogauss<R>(oa.a, oa.p, oa.cx, oa.cy, oa.cz, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j),
-                           pz<R>(v, j));
-      if (!kept(ov.gvolp)) continue;
+  }
+  return lane == 31 || kn != key;
+}
+
+/* one thread per order-M record q: its generating overlap a, its rank k
+   among a's kept children, the k-th kept sibling b (from the mask, or by
+   search), the record itself and its volume terms; the terms of the
+   generator's parents are summed over the warp's run of records sharing
+   the generator before the atomics */
+template <typename R, int M>
+__global__ void k_lm_emit(View v) {
+  if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
+  const int n = min(v.dc[DC_L0 + M], v.cap[M]);
+  const int cm = v.cap[M - 1], cn = v.cap[M];
+  const int lane = threadIdx.x & 31;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long base = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; base < n;
+       base += nwarps * 32) {
+    const int q = (int)base + lane;
+    int a = -1 - lane;
+    double sums[2 * (M - 1)];
 #pragma unroll
-      for (int k = 0; k < M - 1; k++) v.par[M][(size_t)k * cn + q] = par[k];
-      v.par[M][(size_t)(M - 1) * cn + q] = j;
-      rec_put<R>(v, M, q, ov);
-      v.gend[M][q] = qend;
+    for (int k = 0; k < 2 * (M - 1); k++) sums[k] = 0.0;
+    if (q < n) {
+      a = v.lv_own[M][q];
+      const int q0 = v.lv_off[M][a], rank = q - q0, qend = q0 + v.lv_cnt[M][a];
+      const unsigned long long mask = v.lv_mask[M][a];
+      const Ov<R> oa = rec_load<R>(v, M - 1, a);
+      int j = 0;
+      Ov<R> ov;
+      if (mask) {
+        unsigned long long mm = mask;
+        for (int t = 0; t < rank; t++) mm &= mm - 1; /* drop the lower kept siblings */
+        const int b = a + __ffsll((long long)mm);
+        j = v.par[M - 1][(size_t)(M - 2) * cm + b];
+        ov = ogauss<R>(oa.a, oa.p, oa.cx, oa.cy, oa.cz, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j),
+                       pz<R>(v, j));
+      } else {
+        const int ge = v.gend[M - 1][a];
+        int c = -1;
+        for (int b = a + 1; b < ge && c < rank; b++) {
+          j = v.par[M - 1][(size_t)(M - 2) * cm + b];
+          ov = ogauss<R>(oa.a, oa.p, oa.cx, oa.cy, oa.cz, atom_alpha<R>(v, j), R(C_PFC), px<R>(v, j), py<R>(v, j),
+                         pz<R>(v, j));
+          if (kept(ov.gvolp)) c++;
+        }
+      }
       double dv, ds;
 #pragma unroll
       for (int k = 0; k < M - 1; k++) {
-        vol_terms<R, M>(v, par[k], ov, dv, ds);
-        svol[k] += dv;
-        ssurf[k] += ds;
+        const int pk = v.par[M - 1][(size_t)k * cm + a];
+        v.par[M][(size_t)k * cn + q] = pk;
+        vol_terms<R, M>(v, pk, ov, dv, ds);
+        sums[2 * k] = dv;
+        sums[2 * k + 1] = ds;
       }
+      v.par[M][(size_t)(M - 1) * cn + q] = j;
+      rec_put<R>(v, M, q, ov);
+      v.gend[M][q] = qend;
       vol_terms<R, M>(v, j, ov, dv, ds);
       atomicAdd(&v.volumep[j], dv);
       atomicAdd(&v.surf[j], ds);
-      q++;
     }
+    if (seg_scan_n(sums, a) && a >= 0) {
 #pragma unroll
-    for (int k = 0; k < M - 1; k++) {
-      atomicAdd(&v.volumep[par[k]], svol[k]);
-      atomicAdd(&v.surf[par[k]], ssurf[k]);
+      for (int k = 0; k < M - 1; k++) {
+        const int pk = v.par[M - 1][(size_t)k * cm + a];
+        atomicAdd(&v.volumep[pk], sums[2 * k]);
+        atomicAdd(&v.surf[pk], sums[2 * k + 1]);
+      }
     }
   }
 }
@@ -2367,7 +2431,10 @@ static int tree_free(agb_dev *s) {
   for (int m = 2; m <= AGB_MAX_ORDER; m++) {
     if (s->v.lv_cnt[m]) cudaFree(s->v.lv_cnt[m]);
     if (s->v.lv_off[m]) cudaFree(s->v.lv_off[m]);
-    s->v.lv_cnt[m] = s->v.lv_off[m] = NULL;
+    if (s->v.lv_mask[m]) cudaFree(s->v.lv_mask[m]);
+    if (s->v.lv_own[m]) cudaFree(s->v.lv_own[m]);
+    s->v.lv_cnt[m] = s->v.lv_off[m] = s->v.lv_own[m] = NULL;
+    s->v.lv_mask[m] = NULL;
   }
   if (s->v.ws_cand) cudaFree(s->v.ws_cand);
   if (s->v.ws_srt) cudaFree(s->v.ws_srt);
@@ -2425,6 +2492,8 @@ static int tree_alloc(agb_dev *s) {
     /* one count / offset per generating overlap of order m-1 */
     CK(cudaMalloc((void **)&s->v.lv_cnt[m], sizeof(int) * (size_t)s->cap[m - 1]));
     CK(cudaMalloc((void **)&s->v.lv_off[m], sizeof(int) * (size_t)s->cap[m - 1]));
+    CK(cudaMalloc((void **)&s->v.lv_mask[m], sizeof(unsigned long long) * (size_t)s->cap[m - 1]));
+    CK(cudaMalloc((void **)&s->v.lv_own[m], sizeof(int) * (size_t)s->cap[m]));
   }
   s->scan_cap = maxcap > s->cap_nl ? maxcap : s->cap_nl;
   if (s->v.nbuckets > s->scan_cap) s->scan_cap = s->v.nbuckets;
@@ -3153,12 +3222,22 @@ static void launch_all(agb_dev *s, int seg = -1) {
     }
     agb_scan_excl(v.lv_cnt[m], v.lv_off[m], v.dc + DC_L0 + m - 1, v.dc + DC_L0 + m, v.cap[m - 1], s->scan_scratch,
                   st);
+    const int ge = nblocks(v.cap[m]);
     switch (m) {
-      case 3: AGB_LAUNCH((k_lm_emit<R, 3>), g, BLK, st, v); break;
-      case 4: AGB_LAUNCH((k_lm_emit<R, 4>), g, BLK, st, v); break;
-      default: AGB_LAUNCH((k_lm_emit<R, 5>), g, BLK, st, v); break;
+      case 3:
+        AGB_LAUNCH((k_lm_owner<3>), g, BLK, st, v);
+        AGB_LAUNCH((k_lm_emit<R, 3>), ge, BLK, st, v);
+        break;
+      case 4:
+        AGB_LAUNCH((k_lm_owner<4>), g, BLK, st, v);
+        AGB_LAUNCH((k_lm_emit<R, 4>), ge, BLK, st, v);
+        break;
+      default:
+        AGB_LAUNCH((k_lm_owner<5>), g, BLK, st, v);
+        AGB_LAUNCH((k_lm_emit<R, 5>), ge, BLK, st, v);
+        break;
     }
-    nl += 2 + AGB_SCAN_LAUNCHES;
+    nl += 3 + AGB_SCAN_LAUNCHES;
   }
   stage_mark(s, 3);
   AGB_LAUNCH(k_scaling, nblocks(N), BLK, st, v);
