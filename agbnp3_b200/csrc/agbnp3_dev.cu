@@ -391,7 +391,9 @@ __device__ __forceinline__ void for_cell(const View &v, int I, int ax, int ay, i
    the error word and the largest count needed */
 __global__ void k_nl_slab(View v) {
   AGB_GRID_STRIDE(q, 27LL * v.natoms) {
-    int g = (int)(q / 27), c = (int)(q % 27);
+    /* cell-major over the pair slots: the lanes of a warp hold spatially
+       close atoms looking into the same neighbour direction */
+    int c = (int)(q / v.natoms), g = v.slot_atom[(int)(q % v.natoms)];
     int I = v.inst_of[g];
     if (g >= v.inst_begin[I] + v.inst_nheavy[I]) continue;
     f4 a = v.pos[g];
