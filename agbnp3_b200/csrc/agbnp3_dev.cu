@@ -777,22 +777,6 @@ __global__ void k_lm_count(View v) {
   }
 }
 
-/* the generating overlap of every order-M record (one thread per
-   generating overlap; a few records each) */
-template <int M>
-__global__ void k_lm_owner(View v) {
-  if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
-  const int n = min(v.dc[DC_L0 + M - 1], v.cap[M - 1]);
-  AGB_GRID_STRIDE(a, n) {
-    const int q = v.lv_off[M][a], c = v.lv_cnt[M][a];
-    if (q + c > v.cap[M]) {
-      set_err(v, AGB_ERR_TREE_CAP);
-      continue;
-    }
-    for (int k = 0; k < c; k++) v.lv_own[M][q + k] = (int)a;
-  }
-}
-
 /* sum of a[0..NN) over the run of consecutive lanes holding this lane's
    key; returns whether this lane ends its run */
 template <typename T, int NN>
@@ -822,6 +806,9 @@ __device__ __forceinline__ bool seg_scan_n(T (&a)[NN], int key) {
 template <typename R, int M>
 __global__ void k_lm_emit(View v) {
   if (v.dc[DC_ERR] & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP)) return;
+  if (v.dc[DC_L0 + M] > v.cap[M]) { /* the records up to the capacity are still made, then redone */
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_err(v, AGB_ERR_TREE_CAP);
+  }
   const int n = min(v.dc[DC_L0 + M], v.cap[M]);
   const int cm = v.cap[M - 1], cn = v.cap[M];
   const int lane = threadIdx.x & 31;
@@ -3222,24 +3209,16 @@ static void launch_all(agb_dev *s, int seg = -1) {
       case 4: AGB_LAUNCH((k_lm_count<R, 4>), g, BLK, st, v); break;
       default: AGB_LAUNCH((k_lm_count<R, 5>), g, BLK, st, v); break;
     }
-    agb_scan_excl(v.lv_cnt[m], v.lv_off[m], v.dc + DC_L0 + m - 1, v.dc + DC_L0 + m, v.cap[m - 1], s->scan_scratch,
-                  st);
+    /* the scan also maps each new record to its generating overlap */
+    agb_scan_excl_owner(v.lv_cnt[m], v.lv_off[m], v.dc + DC_L0 + m - 1, v.dc + DC_L0 + m, v.cap[m - 1],
+                        s->scan_scratch, st, v.lv_own[m], v.cap[m]);
     const int ge = nblocks(v.cap[m]);
     switch (m) {
-      case 3:
-        AGB_LAUNCH((k_lm_owner<3>), g, BLK, st, v);
-        AGB_LAUNCH((k_lm_emit<R, 3>), ge, BLK, st, v);
-        break;
-      case 4:
-        AGB_LAUNCH((k_lm_owner<4>), g, BLK, st, v);
-        AGB_LAUNCH((k_lm_emit<R, 4>), ge, BLK, st, v);
-        break;
-      default:
-        AGB_LAUNCH((k_lm_owner<5>), g, BLK, st, v);
-        AGB_LAUNCH((k_lm_emit<R, 5>), ge, BLK, st, v);
-        break;
+      case 3: AGB_LAUNCH((k_lm_emit<R, 3>), ge, BLK, st, v); break;
+      case 4: AGB_LAUNCH((k_lm_emit<R, 4>), ge, BLK, st, v); break;
+      default: AGB_LAUNCH((k_lm_emit<R, 5>), ge, BLK, st, v); break;
     }
-    nl += 3 + AGB_SCAN_LAUNCHES;
+    nl += 2 + AGB_SCAN_LAUNCHES;
   }
   stage_mark(s, 3);
   AGB_LAUNCH(k_scaling, nblocks(N), BLK, st, v);

@@ -30,6 +30,10 @@
    in/out and sizes the grid; scratch holds cap/1024+2 ints. */
 void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s);
 #define AGB_SCAN_LAUNCHES 2 /* kernels one agb_scan_excl launches */
+/* the same, also writing owner[out[i] + t] = i for t < in[i] (slots of
+   owner beyond owner_cap are skipped): the item each output belongs to */
+void agb_scan_excl_owner(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s,
+                         int *owner, int owner_cap);
 
 /* out[q*nseg + k] = sum of vals[q*stride + j] for j in [seg[k], seg[k+1]),
    for q < nq; one block per (q, k), fixed reduction order */

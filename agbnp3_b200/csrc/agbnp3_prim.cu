@@ -59,7 +59,8 @@ __device__ __forceinline__ int block_sum(int x, int *sh) {
    (each block adds those tile sums itself: a few hundred ints); the block
    of the last tile writes the total */
 __global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, const int *__restrict__ n, int cap,
-                             const int *__restrict__ tile_sum, int *__restrict__ total) {
+                             const int *__restrict__ tile_sum, int *__restrict__ total, int *__restrict__ owner,
+                             int owner_cap) {
   __shared__ int sh[32];
   const int len = min(*n, cap);
   const long long ntiles = ((long long)len + SCAN_TILE - 1) / SCAN_TILE;
@@ -99,7 +100,12 @@ __global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, 
     int run = prefix + x - s + (warp > 0 ? sh[warp - 1] : 0);
     for (int k = 0; k < SCAN_ITEMS; k++) {
       long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
-      if (i < len) out[i] = run;
+      if (i < len) {
+        out[i] = run;
+        /* the item each output slot belongs to (bounded by owner_cap) */
+        if (owner)
+          for (int t = 0; t < v[k] && run + t < owner_cap; t++) owner[run + t] = (int)i;
+      }
       run += v[k];
     }
     if (tile == ntiles - 1 && threadIdx.x == SCAN_BLOCK - 1) *total = run;
@@ -107,12 +113,17 @@ __global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, 
   }
 }
 
-void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s) {
+void agb_scan_excl_owner(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s,
+                         int *owner, int owner_cap) {
   int ntiles = (cap + SCAN_TILE - 1) / SCAN_TILE;
   if (ntiles < 1) ntiles = 1;
   int grid = ntiles < 148 * 2 ? ntiles : 148 * 2; /* two 1024-thread blocks per SM */
   AGB_LAUNCH(k_scan_tiles, grid, SCAN_BLOCK, s, in, n, cap, scratch);
-  AGB_LAUNCH(k_scan_apply, grid, SCAN_BLOCK, s, in, out, n, cap, scratch, total);
+  AGB_LAUNCH(k_scan_apply, grid, SCAN_BLOCK, s, in, out, n, cap, scratch, total, owner, owner_cap);
+}
+
+void agb_scan_excl(const int *in, int *out, const int *n, int *total, int cap, int *scratch, cudaStream_t s) {
+  agb_scan_excl_owner(in, out, n, total, cap, scratch, s, nullptr, 0);
 }
 
 #define SEG_BLOCK 256
