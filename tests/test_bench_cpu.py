@@ -1,0 +1,53 @@
+"""The benchmark's roofline arithmetic (no GPU): pair counts per launch,
+flop weights, fractions of the measured peak, and the captured DRAM traffic
+reported only for the workload it was captured on."""
+import importlib.util
+import os
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def bench():
+    spec = importlib.util.spec_from_file_location("bench", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+PEAKS = {"fp32_tflops": 72.0, "fp64_tflops": 36.0, "ex2_tops": 4.6, "nominal_sm_mhz": 1965.0}
+
+
+def test_pair_roofline_25k(bench):
+    n, nh = 25000, 12500
+    stage = {"invb": 0.32, "agb": 0.44, "gbders": 0.74}
+    r = bench.pair_roofline(n, nh, stage, PEAKS)
+    # unordered pairs, directed pairs with a heavy descreener, pairs with a heavy atom
+    agb_flops = n * (n - 1) // 2 * bench.PAIR_OPS["agb"][0]
+    invb_flops = (n * nh - nh) * bench.PAIR_OPS["invb"][0]
+    gbd_flops = nh * (nh - 1) // 2 * bench.PAIR_OPS["gbders_hh"][0] + nh * (n - nh) * bench.PAIR_OPS["gbders_hx"][0]
+    st = r["stages"]
+    assert st["agb"]["gflop_per_launch"] == pytest.approx(agb_flops / 1e9)
+    assert st["invb"]["gflop_per_launch"] == pytest.approx(invb_flops / 1e9)
+    assert st["gbders"]["gflop_per_launch"] == pytest.approx(gbd_flops / 1e9)
+    for k, ms in stage.items():
+        assert st[k]["fp32_frac"] == pytest.approx(st[k]["gflop_per_launch"] / (ms * 1e-3) / 1e3 / PEAKS["fp32_tflops"])
+    # the dominant (slowest) pair kernel carries the headline fraction and its captured traffic
+    assert r["kernel"] == "k_gbders_sym" and r["frac"] == st["gbders"]["fp32_frac"]
+    assert r["achieved"] == pytest.approx(r["frac"] * r["peak"])
+    assert r["traffic"] == bench.NCU_TRAFFIC_25K["k_gbders_sym"]
+    tot = sum(st[k]["gflop_per_launch"] for k in stage)
+    assert st["all_pair_stages"]["tflops"] == pytest.approx(tot / (sum(stage.values()) * 1e-3) / 1e3)
+
+
+def test_pair_roofline_other_size_has_no_traffic(bench):
+    r = bench.pair_roofline(100000, 50000, {"invb": 4.0, "agb": 6.7, "gbders": 7.6}, PEAKS)
+    assert r["kernel"] == "k_gbders_sym" and r["traffic"] is None
+    assert 0.0 < r["frac"] < 1.5
+
+
+def test_metric_name(bench):
+    assert bench.metric_name(25000).startswith("energy+grad evals/s @25k atoms")
+    assert "@2500 atoms" in bench.metric_name(2500)
