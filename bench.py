@@ -162,7 +162,8 @@ def reference_arm(args):
     tot = sum(d["times"])
     v = len(d["times"]) / tot
     print(json.dumps({
-        "impl": "reference", "metric": metric_name(args.natoms), "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "impl": "reference", "metric": metric_name(args.natoms), "value": v, "unit": UNIT, "n_gpus": world,
+        "devices": f"host CPU ({threads} threads); the reference has no GPU path", "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(d["times"]), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",

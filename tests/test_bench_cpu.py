@@ -51,3 +51,25 @@ def test_pair_roofline_other_size_has_no_traffic(bench):
 def test_metric_name(bench):
     assert bench.metric_name(25000).startswith("energy+grad evals/s @25k atoms")
     assert "@2500 atoms" in bench.metric_name(2500)
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` on a small globule: one JSON line with the
+    benchmark contract's keys, timing the reference library on host cores."""
+    import json
+    import subprocess
+    import sys
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libagbnp3_ref.so")):
+        pytest.skip("reference library not built")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--natoms", "2000",
+                          "--steps", "2", "--warmup", "1"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["steps"] == 2
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
