@@ -73,3 +73,22 @@ def test_reference_arm_line():
     assert d["impl"] == "reference" and d["value"] > 0 and d["steps"] == 2
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+
+
+def test_ncu_launch_summary(tmp_path):
+    """The launch-list summariser groups kernels by name (template arguments
+    kept apart), converts units and skips ncu's banner lines."""
+    from agbnp3_b200.ncu_summary import kernel_key, summarise
+    hdr = ('"ID","Process ID","Process Name","Host Name","Kernel Name","Context","Stream","Block Size","Grid Size",'
+           '"Device","CC","Section Name","Metric Name","Metric Unit","Metric Value"\n')
+    rows = [("k_prep(View)", "ns", "6,000"), ("void k_tree_ders<float, 3>(View)", "us", "40.5"),
+            ("void k_tree_ders<float, 3>(View)", "us", "39.5"), ("void k_tree_ders<float, 4>(View)", "ns", "1000")]
+    text = "==PROF== Connected\n" + hdr + "".join(
+        f'"{i}","1","py","h","{k}","1","13","(128, 1, 1)","(1, 1, 1)","0","10.0","s","gpu__time_duration.sum","{u}","{v}"\n'
+        for i, (k, u, v) in enumerate(rows))
+    p = tmp_path / "launches.csv"
+    p.write_text(text)
+    tot, cnt = summarise(str(p))
+    assert kernel_key("void k_tree_ders<float, 3>(View)") == "k_tree_ders<float, 3>"
+    assert cnt["k_tree_ders<float, 3>"] == 2 and tot["k_tree_ders<float, 3>"] == pytest.approx(80000.0)
+    assert tot["k_prep"] == pytest.approx(6000.0) and tot["k_tree_ders<float, 4>"] == pytest.approx(1000.0)
