@@ -38,6 +38,10 @@ static void errprint(const char *fmt, ...) {
 
 const char *agbnp3_last_error(void) { return last_error; }
 
+/* for the library's CUDA translation units: record a message as the last
+   error and print it, as errprint does */
+void agb_host_set_error(const char *msg) { errprint("%s", msg); }
+
 typedef struct {
   int in_use;
   int natoms, nheavy;

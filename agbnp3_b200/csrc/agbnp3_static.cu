@@ -18,6 +18,7 @@
  * must be serialised by the caller.  Each call rewrites every scratch entry
  * it reads, so nothing carries over between calls.
  */
+#include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -25,7 +26,6 @@
 
 #define AGBNP3_STATIC_MAX_ATOMS 32768
 #define ST_BLOCK 128
-#define ST_PI 3.14159265359
 #define ST_TOKCAL 332.0
 
 struct __align__(16) st_f4 {
@@ -39,8 +39,23 @@ struct __align__(16) st_f4 {
 static __device__ __align__(256) unsigned char g_static_scratch[ST_BYTES_F4 + ST_BYTES_F2 + ST_BYTES_E];
 
 #define ST_MAX_DEVICES 64
+/* device address of g_static_scratch per device.  Two host threads making
+   their first call on the same device at once both store the same address,
+   so the unsynchronised write is harmless. */
 static void *st_addr[ST_MAX_DEVICES];
-static char st_err[256];
+
+/* sets the library's last-error string (agbnp3_last_error) and prints it */
+extern "C" void agb_host_set_error(const char *msg);
+
+static int st_fail(const char *fmt, ...) {
+  char msg[256];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(msg, sizeof(msg), fmt, ap);
+  va_end(ap);
+  agb_host_set_error(msg);
+  return -1; /* AGBNP_ERR */
+}
 
 __global__ void k_st_pack(int n, const double *x, const double *y, const double *z, const double *q,
                           const double *br, st_f4 *p4, float2 *p2) {
@@ -127,36 +142,21 @@ extern "C" int agbnp3_gb_energy_static(int natoms, const double *x, const double
                                        const double *charge, const double *born_radii, double dielectric_in,
                                        double dielectric_out, double *egb, double *dera, double *dgbdr,
                                        void *stream) {
-  if (natoms <= 0 || natoms > AGBNP3_STATIC_MAX_ATOMS) {
-    snprintf(st_err, sizeof(st_err), "agbnp3_gb_energy_static(): natoms = %d outside 1..%d", natoms,
-             AGBNP3_STATIC_MAX_ATOMS);
-    fprintf(stderr, "%s\n", st_err);
-    return -1;
-  }
-  if (!x || !y || !z || !charge || !born_radii || !egb || !dera || !dgbdr) {
-    snprintf(st_err, sizeof(st_err), "agbnp3_gb_energy_static(): NULL array");
-    fprintf(stderr, "%s\n", st_err);
-    return -1;
-  }
+  if (natoms <= 0 || natoms > AGBNP3_STATIC_MAX_ATOMS)
+    return st_fail("agbnp3_gb_energy_static(): natoms = %d outside 1..%d", natoms, AGBNP3_STATIC_MAX_ATOMS);
+  if (!x || !y || !z || !charge || !born_radii || !egb || !dera || !dgbdr)
+    return st_fail("agbnp3_gb_energy_static(): NULL array");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= ST_MAX_DEVICES) {
-    snprintf(st_err, sizeof(st_err), "agbnp3_gb_energy_static(): no usable current device (%s)",
-             cudaGetErrorString(e));
-    fprintf(stderr, "%s\n", st_err);
-    return -1;
-  }
+  if (e != cudaSuccess || dev < 0 || dev >= ST_MAX_DEVICES)
+    return st_fail("agbnp3_gb_energy_static(): no usable current device (%s)", cudaGetErrorString(e));
   if (!st_addr[dev]) {
     /* the array's name is a host-side stand-in; its device address comes
        from the runtime, per device, with that device current */
     void *p = NULL;
     e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess || !p) {
-      snprintf(st_err, sizeof(st_err), "agbnp3_gb_energy_static(): cudaGetSymbolAddress failed: %s",
-               cudaGetErrorString(e));
-      fprintf(stderr, "%s\n", st_err);
-      return -1;
-    }
+    if (e != cudaSuccess || !p)
+      return st_fail("agbnp3_gb_energy_static(): cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
     st_addr[dev] = p;
   }
   unsigned char *base = (unsigned char *)st_addr[dev];
@@ -170,10 +170,7 @@ extern "C" int agbnp3_gb_energy_static(int natoms, const double *x, const double
   k_st_pair<<<nb, ST_BLOCK, 0, s>>>(natoms, df, p4, p2, eat, dera, dgbdr);
   k_st_sum<<<1, 256, 0, s>>>(natoms, eat, egb);
   e = cudaGetLastError();
-  if (e != cudaSuccess) {
-    snprintf(st_err, sizeof(st_err), "agbnp3_gb_energy_static(): launch failed: %s", cudaGetErrorString(e));
-    fprintf(stderr, "%s\n", st_err);
-    return -1;
-  }
+  if (e != cudaSuccess)
+    return st_fail("agbnp3_gb_energy_static(): launch failed: %s", cudaGetErrorString(e));
   return 2; /* AGBNP_OK */
 }

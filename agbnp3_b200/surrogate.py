@@ -22,7 +22,7 @@ import time
 import numpy as np
 import torch
 
-from . import AGBNP_OK, AGBNPError, Instance, PREC_FP64, lib, make_globule
+from . import AGBNP_OK, AGBNPError, Instance, PREC_FP64, last_error, lib, make_globule
 
 NIN, NH, NOUT = 160, 128, 2
 CLASS_RADII = (1.7, 1.55, 1.52, 1.8, 1.15)  # C, N, O, S, H (A, without the 0.5 A increment)
@@ -285,9 +285,17 @@ def born_radii(S, radius):
     return 1.0 / bf
 
 
+# largest system agbnp3_gb_energy_static accepts (the size of its static
+# device scratch array)
+STATIC_MAX_ATOMS = 32768
+
+
 def gb_energy(system, int2ext, radii_b):
     """GB energy (kcal/mol) of the system (internal order) at the given Born
-    radii, by the library's GB pair kernel (agbnp3_gb_energy_static)"""
+    radii, by the library's allocation-free GB pair kernel
+    (agbnp3_gb_energy_static), which takes at most STATIC_MAX_ATOMS atoms."""
+    if not 0 < system.natoms <= STATIC_MAX_ATOMS:
+        raise AGBNPError(f"gb_energy: {system.natoms} atoms; agbnp3_gb_energy_static takes 1..{STATIC_MAX_ATOMS}")
     L = lib()
     vp = ctypes.c_void_p
     L.agbnp3_gb_energy_static.argtypes = [ctypes.c_int] + [vp] * 5 + [ctypes.c_double] * 2 + [vp] * 3 + [vp]
@@ -302,7 +310,7 @@ def gb_energy(system, int2ext, radii_b):
     rc = L.agbnp3_gb_energy_static(n, *(_p(a) for a in args), system.eps_in, system.eps_out, _p(e), _p(dera),
                                    _p(grad), None)
     if rc != AGBNP_OK:
-        raise AGBNPError("agbnp3_gb_energy_static failed")
+        raise AGBNPError(f"agbnp3_gb_energy_static failed: {last_error()}")
     torch.cuda.synchronize()
     return e.item()
 
