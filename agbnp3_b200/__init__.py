@@ -333,6 +333,14 @@ class Instance:
         a, m = self.debug_fetch(2 + 16 * order, order * n + 1)
         return a[: order * m].reshape(order, m).T.copy()
 
+    def water_sites(self):
+        """(positions [nws, 3], volume scaling factors [nws]) of the water
+        sites of the last evaluation, in the reference's site order."""
+        n = self.stats()["water_sites"]
+        sp, m = self.debug_fetch(200, n + 1, np.float64)
+        pos, _ = self.debug_fetch(201, 3 * n + 3, np.float64)
+        return pos[: 3 * m].reshape(m, 3), sp[:m]
+
     def atom_array(self, k: int):
         a, _ = self.debug_fetch(100 + k, self.natoms, np.float64)
         return a[: self.natoms]

@@ -5,7 +5,7 @@ agbnp3.h:77-104) on seeded synthetic globules.
 
 Run from the repository root where the reference sources are available:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref REF=<reference source tree> && python tests/golden/make_golden.py [names]
 
 Each fixture (npz) holds the system in the caller's atom order, the
 reference's outputs (energies, Born radii, volume scaling factors, surface
@@ -13,6 +13,9 @@ areas, the four gradient arrays) and internal state read by
 oracle/ref_harness.c: the heavy-atom near list, the Gaussian-overlap
 candidates of the overlap tree (raw/switched volumes in enumeration order),
 the water sites and per-atom intermediates.
+
+The large case (25,000 atoms) keeps digests of the index sets and a sample
+of the per-atom outputs instead of whole arrays (see LARGE_CASES).
 
 The reference runs with OMP_NUM_THREADS=1 (its HB energy depends on the
 thread count) and with one instance per process: a second instance in the
@@ -121,14 +124,83 @@ def run_case(args):
     return name, ncand, len(ws["sp"])
 
 
+# large cases: too big to store whole, so the fixture holds digests of the
+# index sets (tests/conftest.py index_set_digest), the reference's kept
+# flags per candidate, the water sites, the energies and the per-atom
+# outputs of a seeded sample of atoms; the system itself is regenerated
+# from (natoms, seed) and pinned by a digest
+LARGE_CASES = [
+    # name, natoms, seed, sampled atoms
+    ("globule25000", 25000, 1, 2000),
+]
+
+
+def run_large_case(args):
+    name, natoms, seed, nsample = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle as O
+    from conftest import array_digest, index_set_digest
+    from agbnp3_b200.system import make_globule
+    s = make_globule(natoms, seed)
+    ref = O.RefLib(harness=True)
+    tag = ref.new(s)
+    R = ref.ener(tag, s)
+    assert R["rc"] == 2, R["rc"]
+    Q = O.oracle_eval(s, internals=True, cand_cap=8_000_000)
+    ncand = Q["cand_total"]
+    v3, v3p = ref.gbuffers(tag, ncand)
+    assert len(v3p) == ncand
+    kept_ref = v3p > np.float32(1.1754944e-38)
+    c = Q["cand"]
+    kept_orc = c["gvolp"] > np.finfo(np.float32).tiny
+    flips = np.nonzero(kept_ref != kept_orc)[0]
+    cnt, nb = ref.near_list(tag, s.nheavy)
+    ws = ref.water_sites(tag)
+    idx = np.sort(np.random.default_rng(seed + 7).choice(natoms, nsample, replace=False))
+    d = dict(
+        natoms=natoms, seed=seed,
+        system_digest=np.array(array_digest(np.concatenate([s.x, s.y, s.z, s.r, s.charge]), "f8")),
+        energies=np.array([R[k] for k in ("egb", "evdw", "ecorr_vdw", "ecav", "ecorr_cav", "ehb", "mol_volume")]),
+        nl_count=cnt, nl_total=np.array(len(nb)), nl_digest=np.array(array_digest(nb, "i4")),
+        ncand=np.array(ncand), cand_kept=np.packbits(kept_ref),
+        # candidates whose keep decision differs between the FP32 reference
+        # and the FP64 oracle (volumes on the switch's lower edge)
+        kept_flips=flips.astype(np.int32), kept_flips_gvol=c["gvol"][flips],
+        ws_pos=ws["pos"], ws_sp=ws["sp"], ws_parent0=ws["parent0"], ws_type=ws["type"],
+        sample=idx.astype(np.int32),
+    )
+    for m in range(2, 6):
+        sel = (c["order"] == m) & kept_ref
+        d[f"kept{m}_count"] = np.array(int(sel.sum()))
+        d[f"kept{m}_digest"] = np.array(index_set_digest(c["parents"][sel, :m]))
+        # the same set with the FP64 oracle's keep decisions
+        sel64 = (c["order"] == m) & kept_orc
+        d[f"kept{m}_fp64_digest"] = np.array(index_set_digest(c["parents"][sel64, :m]))
+    for k in ("sp", "br", "surf_area", "dgbdr", "dvwdr", "decav", "dehb"):
+        d["sample_" + k] = R[k][idx]
+    np.savez_compressed(os.path.join(OUT, name + ".npz"), **d)
+    return name, ncand, len(ws["sp"]), len(flips)
+
+
 def _child(args):
     print("wrote", run_case(args), flush=True)
 
 
+def _child_large(args):
+    print("wrote", run_large_case(args), flush=True)
+
+
 if __name__ == "__main__":
     ctx = mp.get_context("spawn")
-    for case in CASES:
-        p = ctx.Process(target=_child, args=(case,))
+    only = sys.argv[1:]
+    jobs = [(_child, c) for c in CASES] + [(_child_large, c) for c in LARGE_CASES]
+    for fn, case in jobs:
+        if only and case[0] not in only:
+            continue
+        p = ctx.Process(target=fn, args=(case,))
         p.start()
         p.join(timeout=600)
         if p.is_alive():

@@ -166,6 +166,43 @@ def test_batch_matches_members(engine, prec):
             i.close()
 
 
+@pytest.fixture(scope="module")
+def batch64(engine):
+    """64 instances of the batched configuration's distribution: atom counts
+    log-uniform in [300, 5000], 0.2 A coordinate noise, distinct seeds; with
+    the FP64 oracle of every member."""
+    rng = np.random.default_rng(64)
+    sizes = np.exp(rng.uniform(np.log(300), np.log(5000), 64)).astype(int)
+    systems = [A.make_globule(int(n), 5000 + k, noise=0.2) for k, n in enumerate(sizes)]
+    return systems, [O.oracle_eval(x, compat=True) for x in systems]
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+def test_batch64_members_vs_oracle(batch64, prec):
+    """One batched evaluation of 64 uneven instances: every member's
+    energies, per-atom outputs and forces against its own FP64 oracle, at
+    the tolerances of the single-instance parity tests."""
+    systems, oracles = batch64
+    insts = [A.Instance(x, precision=prec) for x in systems]
+    B = A.Batch(insts)
+    B.set_mode(prec, True)
+    t = TOL[prec]
+    try:
+        B.set_coords(np.concatenate([x.coords() for x in systems]))
+        B.ener_resident()
+        R = B.results()
+        for k, Q in enumerate(oracles):
+            o0, o1 = B.offsets[k], B.offsets[k + 1]
+            for e in ENERGY_KEYS:
+                assert abs(R[e][k] - Q[e]) <= t["e"] * max(abs(Q[e]), 10.0), (k, e, R[e][k], Q[e])
+            for g in ("sp", "br", "surf_area", "dgbdr", "dvwdr", "decav", "dehb"):
+                assert rms_rel(R[g][o0:o1], Q[g]) <= t["g"], (k, g, rms_rel(R[g][o0:o1], Q[g]))
+    finally:
+        B.close()
+        for i in insts:
+            i.close()
+
+
 def test_caller_order_and_permutation(engine):
     """Outputs follow the caller's atom order.  AGBNP3 itself depends on
     the atom numbering (the overlap tree is rooted at the lowest index and,
@@ -233,13 +270,22 @@ def test_api_errors_on_device(engine):
         A.delete(tag)
 
 
-@pytest.mark.parametrize("natoms,seed", [(25000, 1)])
-def test_large_fp64_vs_oracle(engine, natoms, seed):
-    """The benchmark workload (25,000-atom globule): plain FP64 path against
-    the FP64 oracle, and the mixed path within the model's accuracy targets
-    (energy 1e-4 relative, forces 1e-3 RMS relative)."""
-    s = A.make_globule(natoms, seed)
-    Q = O.oracle_eval(s, compat=True)
+@pytest.fixture(scope="module")
+def large25k(engine):
+    """The benchmark workload (25,000-atom globule, seed 1), its reference
+    fixture (digests of the index sets, energies, water sites, sampled
+    per-atom outputs) and the FP64 oracle with its overlap candidates."""
+    from conftest import load_large_golden
+    s, d = load_large_golden("globule25000")
+    Q = O.oracle_eval(s, compat=True, internals=True, cand_cap=int(d["ncand"]) + 10)
+    return s, d, Q
+
+
+def test_large_fp64_vs_oracle(large25k):
+    """25,000 atoms: plain FP64 path against the FP64 oracle, and the mixed
+    path within the model's accuracy targets (energy 1e-4 relative, forces
+    1e-3 RMS relative)."""
+    s, d, Q = large25k
     a = A.Instance(s, precision=A.PREC_FP64)
     b = A.Instance(s, precision=A.PREC_MIXED)
     try:
@@ -252,6 +298,57 @@ def test_large_fp64_vs_oracle(engine, natoms, seed):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+def test_large_vs_reference_golden(large25k, prec):
+    """25,000 atoms, through agbnp3_ener, against the reference library run
+    on the same input (tests/golden/globule25000.npz):
+    - near list (agbnp3.c:3978-4115): bit-exact (counts, and the digest of
+      the concatenated lists in the reference's order);
+    - kept overlaps of orders 2-5 (agbnp3_cpu_simd_kernels.c:1064-1598): in
+      FP64 the same sets as the FP64 oracle, whose sets the fixture pins
+      (digest; they differ from the FP32 reference's only by the candidates
+      on the switch's lower edge that the fixture lists); in the mixed mode
+      the same sets up to candidates on that edge;
+    - water sites (agbnp3.c:1837-3761): same count, positions 1e-4 A,
+      scaling factors 1e-5;
+    - energies within 2e-5 relative, sampled per-atom outputs at the FP32
+      tolerances of the golden tests."""
+    from conftest import array_digest, index_set_digest
+    s, d, Q = large25k
+    inst = A.Instance(s, precision=prec, compat=True)
+    try:
+        R = inst.ener()
+        cnt, lst = inst.near_list()
+        assert np.array_equal(cnt[: s.nheavy], d["nl_count"])
+        assert len(lst) == int(d["nl_total"]) and array_digest(lst, "i4") == str(d["nl_digest"])
+        c = Q["cand"]
+        for m in range(2, 6):
+            got = inst.overlaps(m)
+            if prec == A.PREC_FP64:
+                assert index_set_digest(got) == str(d[f"kept{m}_fp64_digest"]), m
+            else:
+                sel = (c["order"] == m) & (c["gvolp"] > np.finfo(np.float32).tiny)
+                diff = canonical(c["parents"][sel, :m]) ^ canonical(got)
+                if diff:
+                    om = c["order"] == m
+                    border = {tuple(sorted(p)) for p, g in zip(c["parents"][om, :m].tolist(), c["gvol"][om])
+                              if abs(g - 0.01) < 1e-5}
+                    assert diff <= border, (m, len(diff))
+        pos, wsp = inst.water_sites()
+        assert len(wsp) == len(d["ws_sp"])
+        assert np.abs(pos - d["ws_pos"]).max() < 1e-4
+        assert np.abs(wsp - d["ws_sp"]).max() < 1e-5
+        for k, ref in zip(ENERGY_KEYS, d["energies"]):
+            assert abs(R[k] - ref) <= 2e-5 * max(abs(ref), 1.0), (k, R[k], ref)
+        idx = d["sample"]
+        for k in ("sp", "br", "surf_area"):
+            assert rms_rel(R[k][idx], d["sample_" + k]) < 2e-5, k
+        for k in ("dgbdr", "dvwdr", "decav", "dehb"):
+            assert rms_rel(R[k][idx], d["sample_" + k]) < 1e-4, (k, rms_rel(R[k][idx], d["sample_" + k]))
+    finally:
+        inst.close()
 
 
 def test_mixed_100k_against_fp64(engine):

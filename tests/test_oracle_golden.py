@@ -132,3 +132,62 @@ def test_oracle_finite_differences(compat):
     else:
         assert worst["ecav"] < 1e-5, worst
         assert 1e-4 < worst["egb"] < 5e-2, worst
+
+
+@pytest.fixture(scope="module")
+def large():
+    from conftest import load_large_golden
+    s, d = load_large_golden("globule25000")
+    q = O.oracle_eval(s, compat=True, internals=True, cand_cap=int(d["ncand"]) + 10)
+    return s, d, q
+
+
+def test_large_energies_and_sample(large):
+    """25,000-atom globule: energies and the sampled per-atom outputs of the
+    reference against the FP64 oracle, at the FP32 tolerances above."""
+    s, d, q = large
+    for k, ref in zip(ENERGY_KEYS, d["energies"]):
+        assert abs(q[k] - ref) <= E_REL * max(abs(ref), 1.0), (k, q[k], ref)
+    idx = d["sample"]
+    for k in ("sp", "br", "surf_area"):
+        assert rms_rel(q[k][idx], d["sample_" + k]) < A_RMS, k
+    for k in ("dgbdr", "dvwdr", "decav", "dehb"):
+        assert rms_rel(q[k][idx], d["sample_" + k]) < G_RMS, (k, rms_rel(q[k][idx], d["sample_" + k]))
+
+
+def test_large_index_sets(large):
+    """25,000-atom globule: the oracle's near list and overlap candidates
+    against the reference's (agbnp3.c:3978-4115,
+    agbnp3_cpu_simd_kernels.c:1064-1598).  The near list is bit-exact; the
+    keep decisions differ only where the raw volume sits on the switch's
+    lower edge (0.01 A^3); the kept sets' digests follow."""
+    from conftest import array_digest, index_set_digest
+    s, d, q = large
+    it = q["int"]
+    assert np.array_equal(it["nl_count"], d["nl_count"])
+    assert len(it["nl_list"]) == int(d["nl_total"])
+    assert array_digest(it["nl_list"], "i4") == str(d["nl_digest"])
+    n = int(d["ncand"])
+    assert q["cand_total"] == n
+    c = q["cand"]
+    kept_ref = np.unpackbits(d["cand_kept"])[:n].astype(bool)
+    kept = c["gvolp"] > np.finfo(np.float32).tiny
+    diff = np.nonzero(kept != kept_ref)[0]
+    assert np.array_equal(diff, d["kept_flips"])
+    assert np.all(np.abs(c["gvol"][diff] - 0.01) < 1e-6), c["gvol"][diff]
+    for m in range(2, 6):
+        sel = (c["order"] == m) & kept
+        assert index_set_digest(c["parents"][sel, :m]) == str(d[f"kept{m}_fp64_digest"]), m
+        sel_ref = (c["order"] == m) & kept_ref
+        assert int(sel_ref.sum()) == int(d[f"kept{m}_count"])
+        assert index_set_digest(c["parents"][sel_ref, :m]) == str(d[f"kept{m}_digest"]), m
+
+
+def test_large_water_sites(large):
+    s, d, q = large
+    it = q["int"]
+    assert q["nws"] == len(d["ws_sp"])
+    assert np.array_equal(it["ws_type"], d["ws_type"])
+    assert np.array_equal(it["ws_parent0"], d["ws_parent0"])
+    assert np.abs(it["ws_pos"] - d["ws_pos"]).max() < 1e-4
+    assert np.abs(it["ws_sp"] - d["ws_sp"]).max() < 1e-5
