@@ -1389,12 +1389,12 @@ __device__ __forceinline__ T rot1(T x) {
    occupancy) */
 template <typename R>
 struct SymNI {
-  static constexpr int agb = sizeof(R) == 4 ? 3 : 2;
+  /* FP32: four i atoms, two packed pairs of k_agb_x2 */
+  static constexpr int agb = sizeof(R) == 4 ? 4 : 2;
   static constexpr int gbd = sizeof(R) == 4 ? 4 : 2;
-  /* resident 128-thread blocks per SM asked of the GB pair pass in FP32:
-     three i atoms per lane at 72 registers (7 blocks) measured faster than
-     four at 95 (5 blocks, 4 % slower) or 80 (6 blocks, 2 % slower) */
-  static constexpr int agb_blocks = sizeof(R) == 4 ? 7 : 1;
+  /* resident 128-thread blocks per SM asked of the scalar GB pair pass in
+     FP32 (kept for comparison, AGBNP3_PAIR_SCALAR=1) */
+  static constexpr int agb_blocks = sizeof(R) == 4 ? 5 : 1;
 };
 #define AGB_NI (SymNI<R>::agb)
 
@@ -1698,6 +1698,8 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
     }
   }
 }
+
+#include "agbnp3_pairx2.cuh"
 
 /* U_i, V_i normalised by the atomic volume and the surface-area effective
    gammas (agbnp3_cpu_simd_kernels.c:861-874) */
@@ -2370,6 +2372,7 @@ struct agb_dev {
   int4 *items_agb, *items_gbd; /* (instance, i tile, first j tile, j tiles) */
   int n_agb, n_gbd;
   int tiled_pairs; /* use the one-sided tiled pair kernels instead */
+  int scalar_pairs; /* FP32: the scalar symmetric pair kernels instead of the packed f32x2 ones */
   int jb;          /* j tiles per symmetric work item */
   int items_prec;  /* precision the symmetric items were built for (i block size) */
   int sfeat_ready; /* the feature kernel's shared-memory limit is set */
@@ -2837,6 +2840,8 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   {
     const char *tp = getenv("AGBNP3_PAIR_TILED");
     s->tiled_pairs = tp && atoi(tp) != 0;
+    const char *sp = getenv("AGBNP3_PAIR_SCALAR");
+    s->scalar_pairs = sp && atoi(sp) != 0;
     int nch = 0, jb = 8;
     const char *e1 = getenv("AGBNP3_DESC_CHUNKS"), *e2 = getenv("AGBNP3_SYM_RUN");
     if (e1) nch = atoi(e1);
@@ -3248,6 +3253,8 @@ static void launch_all(agb_dev *s, int seg = -1) {
   stage_mark(s, 5);
   if (s->tiled_pairs)
     AGB_LAUNCH(k_agb_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  else if (sizeof(R) == 4 && !s->scalar_pairs)
+    AGB_LAUNCH(k_agb_x2, sym_grid(s->n_agb), 128, st, v, s->items_agb, s->n_agb);
   else
     AGB_LAUNCH(k_agb_sym<R>, sym_grid(s->n_agb), 128, st, v, s->items_agb, s->n_agb);
   nl += 1;
@@ -3259,6 +3266,10 @@ static void launch_all(agb_dev *s, int seg = -1) {
   stage_mark(s, 6);
   if (s->tiled_pairs)
     AGB_LAUNCH(k_gbders_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
+  else if (sizeof(R) == 4 && !s->scalar_pairs && s->compat)
+    AGB_LAUNCH(k_gbders_x2<true>, sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
+  else if (sizeof(R) == 4 && !s->scalar_pairs)
+    AGB_LAUNCH(k_gbders_x2<false>, sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
   else if (s->compat)
     AGB_LAUNCH((k_gbders_sym<R, true>), sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
   else

@@ -2,6 +2,13 @@
 per kernel: launches, total device time and share of the total.
 
     python -m agbnp3_b200.ncu_summary launches.csv [--evals N]
+    python -m agbnp3_b200.ncu_summary capture.csv --evals N --traffic-json out.json \
+        --command "<the ncu command>" --workload "<what it ran>"
+
+With --traffic-json the capture must also hold dram__bytes_read.sum and
+dram__bytes_write.sum; the file lists per kernel its launches and DRAM
+bytes per launch and per evaluation (bench.py reads it for the roofline's
+traffic figures).
 
 Kernel names are grouped without their template arguments' values kept
 apart (``k_tree_ders<float, 3>`` and ``<float, 5>`` stay separate, the
@@ -14,6 +21,7 @@ absolute times.
 import argparse
 import collections
 import csv
+import json
 import re
 
 
@@ -23,27 +31,60 @@ def kernel_key(name: str) -> str:
     return name.strip()
 
 
-def summarise(path: str):
-    tot = collections.defaultdict(float)
-    cnt = collections.Counter()
+TIME_SCALE = {"ns": 1.0, "nsecond": 1.0, "us": 1e3, "usecond": 1e3, "ms": 1e6, "msecond": 1e6}
+BYTE_SCALE = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}
+
+
+def _rows(path: str):
     with open(path) as f:
         lines = [ln for ln in f if ln.startswith('"')]
-    for r in csv.DictReader(lines):
+    return list(csv.DictReader(lines))
+
+
+def summarise(path: str):
+    """total device time (ns) and launch count per kernel"""
+    tot = collections.defaultdict(float)
+    cnt = collections.Counter()
+    for r in _rows(path):
         if r.get("Metric Name") != "gpu__time_duration.sum":
             continue
         v = float(r["Metric Value"].replace(",", ""))
-        scale = {"ns": 1.0, "us": 1e3, "usecond": 1e3, "ms": 1e6, "msecond": 1e6}.get(r["Metric Unit"], 1.0)
         k = kernel_key(r["Kernel Name"])
-        tot[k] += v * scale
+        tot[k] += v * TIME_SCALE.get(r["Metric Unit"], 1.0)
         cnt[k] += 1
     return tot, cnt
+
+
+def traffic(path: str, evals: int):
+    """per kernel: launches, DRAM bytes (dram__bytes_read.sum +
+    dram__bytes_write.sum) per launch and per evaluation, device time per
+    launch, from a capture with those metrics"""
+    tot, cnt = summarise(path)
+    dram = collections.defaultdict(float)
+    for r in _rows(path):
+        if r.get("Metric Name") not in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            continue
+        v = float(r["Metric Value"].replace(",", ""))
+        dram[kernel_key(r["Kernel Name"])] += v * BYTE_SCALE.get(r["Metric Unit"], 1.0)
+    out = {}
+    for k in cnt:
+        out[k] = {"launches_per_eval": cnt[k] / evals, "dram_bytes_per_launch": dram[k] / cnt[k],
+                  "dram_bytes_per_eval": dram[k] / evals, "us_per_launch": tot[k] / cnt[k] / 1e3}
+    return out
 
 
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("csv")
     p.add_argument("--evals", type=int, default=1)
+    p.add_argument("--traffic-json", help="write per-kernel DRAM traffic (needs the dram__bytes metrics) here")
+    p.add_argument("--command", default="", help="the profiled command, recorded in the traffic file")
+    p.add_argument("--workload", default="", help="the profiled workload, recorded in the traffic file")
     a = p.parse_args()
+    if a.traffic_json:
+        with open(a.traffic_json, "w") as f:
+            json.dump({"command": a.command, "workload": a.workload, "evals": a.evals,
+                       "kernels": traffic(a.csv, a.evals)}, f, indent=1, sort_keys=True)
     tot, cnt = summarise(a.csv)
     all_ns = sum(tot.values())
     print(f"{'kernel':44s} {'launches':>9s} {'total us':>10s} {'share':>7s}")

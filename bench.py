@@ -35,6 +35,11 @@ def metric_name(natoms):
 UNIT = "evals/s"
 
 
+def workload_name(natoms, nheavy, seed):
+    """config.workload of both arms for the single-globule workloads"""
+    return f"globule {natoms} atoms ({nheavy} heavy), 0.05 heavy/A^3, seed {seed}"
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -46,6 +51,9 @@ def parse():
     p.add_argument("--fp64-steps", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-single-core", action="store_true", help="skip the 1-thread reference timing")
+    p.add_argument("--cpu-best-of", type=int, default=3, help="reference evaluations per CPU baseline timing")
+    p.add_argument("--no-batch", action="store_true", help="skip the 512-instance batch sub-measurement")
+    p.add_argument("--batch-steps", type=int, default=20, help="timed steps of the batch sub-measurement")
     p.add_argument("--config", default="globule25k", choices=["globule25k", "globule100k", "batch512"],
                    help="globule25k: one 25,000-atom globule (headline); globule100k: one 100,000-atom globule "
                         "(per-term error of the chosen mode against the FP64 path); batch512: 512 instances of "
@@ -152,7 +160,9 @@ def reference_arm(args):
     if rank != 0:
         return
     ref_lib = os.path.join(ROOT, "oracle", "_ref", "libagbnp3_ref.so")
-    cfg = {"workload": f"globule {args.natoms} atoms, seed {args.seed}", "natoms": args.natoms}
+    from agbnp3_b200.system import make_globule
+    nheavy = make_globule(args.natoms, args.seed).nheavy
+    cfg = {"workload": workload_name(args.natoms, nheavy, args.seed), "natoms": args.natoms}
     if not os.path.exists(ref_lib):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libagbnp3_ref.so not built "
                           "(needs the reference sources at build time)"}))
@@ -186,11 +196,67 @@ def reference_arm(args):
 PAIR_OPS = {"invb": (18, 1), "agb": (37, 2), "gbders_hh": (29 + 2 * 28, 1), "gbders_hx": (29 + 28, 1)}
 
 
-# DRAM bytes (read + write) per launch of the pair kernels, from the ncu
-# capture of the 25,000-atom globule (profiles/pair_kernels_globule25k_mixed.md;
-# ncu counters cannot be read inside the timed run); reported for that
-# workload only
-NCU_TRAFFIC_25K = {"k_gbders_sym": 2_728_960, "k_agb_sym": 2_025_216, "k_descreen_t": 1_075_200}
+# DRAM traffic per launch of each kernel, read from an ncu capture of the
+# 25,000-atom workload (`python -m agbnp3_b200.ncu_summary --traffic-json`);
+# ncu counters cannot be read inside the timed run, so the traffic is
+# reported for that workload only
+TRAFFIC_JSON = os.path.join(ROOT, "profiles", "dram_traffic_globule25k_mixed.json")
+
+
+def load_traffic(natoms):
+    if natoms != 25000 or not os.path.exists(TRAFFIC_JSON):
+        return None
+    with open(TRAFFIC_JSON) as f:
+        return json.load(f)
+
+
+# kernels of each O(N) stage (name prefixes)
+STAGE_KERNELS = {"nblist": ("k_cell_", "k_nl_", "k_skin_", "k_cand_"),
+                 "volumes": ("k_l2_", "k_lm_", "agb_scan", "k_scan"),
+                 "ws": ("k_ws_",), "treeders": ("k_tree_ders",)}
+
+
+def tree_roofline(natoms, nheavy, counts, stage_ms, hbm_gbs, rbytes, traffic):
+    """The O(N) stages against the HBM roofline.  Algorithmic bytes per
+    evaluation = what the stage must read and write at least once:
+      nblist:   heavy-atom positions and radii (16 B each) in; near-list
+                entries (index + float d^2, 8 B) and per-atom count/offset
+                (8 B) out;
+      volumes:  near-list entries (4 B) and per-atom Gaussian operands
+                (x, y, z, exponent, 1/R: 5 R) in; per kept overlap one
+                12-slot record (12 R) and its parents (4 B each) out, plus
+                the per-atom volume and area (16 B);
+      ws:       positions of all atoms (3 R) and heavy-atom scaling
+                factors (8 B) in; per water site its position (3 R), its
+                3x3 Jacobians to up to four parents (36 R), its scaling
+                factor and HB energy (16 B) out;
+      treeders: every kept record and its parents in, per heavy atom the
+                four chain-rule factors (32 B) in, per atom four gradient
+                rows (96 B) out.
+    R is the working precision's size (4 mixed, 8 FP64)."""
+    R = rbytes
+    P = counts["near_pairs"]
+    K = counts["kept"]
+    nws = counts["water_sites"]
+    rec = sum(k * (12 * R + 4 * m) for m, k in zip(range(2, 6), K))
+    alg = {"nblist": 16 * nheavy + 8 * P + 8 * nheavy,
+           "volumes": 4 * P + 5 * R * natoms + rec + 16 * nheavy,
+           "ws": 3 * R * natoms + 8 * nheavy + nws * (39 * R + 16),
+           "treeders": rec + 32 * nheavy + 96 * natoms}
+    out = {}
+    for k, b in alg.items():
+        t = stage_ms.get(k)
+        if not t:
+            continue
+        gbs = b / (t * 1e-3) / 1e9
+        e = {"alg_bytes": b, "ms": t, "achieved_gbs": gbs, "frac_of_hbm": gbs / hbm_gbs}
+        if traffic:
+            dram = sum(v["dram_bytes_per_eval"] for n, v in traffic["kernels"].items()
+                       if n.startswith(STAGE_KERNELS[k]))
+            e["dram_bytes_ncu"] = dram
+            e["dram_over_alg"] = dram / b
+        out[k] = e
+    return out
 
 
 def pair_roofline(natoms, nheavy, stage_ms, peaks):
@@ -215,14 +281,25 @@ def pair_roofline(natoms, nheavy, stage_ms, peaks):
     dom = max(work, key=lambda k: stages[k]["ms"])
     d = stages[dom]
     kern = {"gbders": "k_gbders_sym", "agb": "k_agb_sym", "invb": "k_descreen_t"}[dom]
-    traffic = NCU_TRAFFIC_25K.get(kern) if natoms == 25000 else None
+    tr = load_traffic(natoms)
+    traffic = tr["kernels"][kern]["dram_bytes_per_launch"] if tr and kern in tr["kernels"] else None
     return {"kernel": kern,
             "stage": dom, "bound": "fp32", "achieved": d["tflops"], "peak": peaks["fp32_tflops"],
             "unit": "TFLOP/s", "frac": d["fp32_frac"], "traffic": traffic,
-            "traffic_note": "DRAM bytes per launch from the ncu capture in profiles/pair_kernels_globule25k_mixed.md "
-                            "(per-atom operands read once, per-atom sums written once)" if traffic else None,
+            "traffic_note": f"DRAM bytes per launch, ncu capture of this workload ({tr['command']})" if traffic else None,
             "peak_source": "measured in this run: FP32 FMA chains on every SM (agbnp3_measure_peaks)",
             "sfu_frac": d["sfu_frac"], "peaks": peaks, "stages": stages}
+
+
+def measured_hbm_gbs():
+    """HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json, written
+    by the pool's own measurement), else the pool's earlier fallback figure"""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return {"gbs": float(json.load(f)["hbm_gbs"]), "source": "measured (MEASURED_PEAKS.json hbm_gbs)"}
+    except (OSError, KeyError, ValueError):
+        return {"gbs": 6650.0, "source": "fallback 6.65 TB/s"}
 
 
 def batch_systems(A, ninst, seed, rank=0):
@@ -233,11 +310,11 @@ def batch_systems(A, ninst, seed, rank=0):
     return [A.make_globule(int(n), rs * 100003 + k, noise=0.2) for k, n in enumerate(sizes)]
 
 
-def batch_main(args, A, torch, rank, world, local):
-    """512 independent instances (log-uniform 300-5,000 atoms, 0.2 A noise)
-    evaluated together: one step = one batched evaluation of all instances;
-    the metric is instance evaluations per second."""
-    systems = batch_systems(A, args.ninst, args.seed, rank)
+def measure_batch(A, torch, ninst, steps, warmup, seed, rank, world, local, clocks=True):
+    """Builds the batched configuration (ninst instances, log-uniform
+    300-5,000 atoms, 0.2 A noise), tunes it and times `steps` batched
+    evaluations (L2 flushed between them); returns the measurements."""
+    systems = batch_systems(A, ninst, seed, rank)
     insts = [A.Instance(x, precision=A.PREC_MIXED) for x in systems]
     B = A.Batch(insts)
     B.set_mode(A.PREC_MIXED, True)
@@ -247,30 +324,34 @@ def batch_main(args, A, torch, rank, world, local):
     tune = B.autotune()
     stream = torch.cuda.ExternalStream(B.stream, device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         B.ener_resident()
     times = []
-    with Clocks(local) as clk:
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-            B.ener_resident()
-            with torch.cuda.stream(stream):
-                e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1))
+    clk = Clocks(local) if clocks else None
+    if clk:
+        clk.__enter__()
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        B.ener_resident()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    if clk:
+        clk.__exit__()
     from agbnp3_b200.shard import max_over_ranks, throughput
     tot = max_over_ranks(sum(times), world, f"cuda:{local}")
-    value = throughput(args.ninst * args.steps, tot / 1e3, world)
+    value = throughput(ninst * steps, tot / 1e3, world)
     B.stage_timing(True)
     B.ener_resident()
     stage_ms = B.stage_times()
     B.stage_timing(False)
     # e2e: host coordinates in, all outputs out, every step
     e2e = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         t0 = time.perf_counter()
         B.set_coords(xyz)
         B.ener_resident()
@@ -280,31 +361,40 @@ def batch_main(args, A, torch, rank, world, local):
     launches = int(B.stats()["launches"])
     # accuracy of the batched mixed path against the FP64 path on 8 members
     acc = []
-    for k in range(0, args.ninst, max(1, args.ninst // 8)):
+    for k in range(0, ninst, max(1, ninst // 8)):
         a = A.Instance(systems[k], precision=A.PREC_FP64)
         F = a.ener()
         e_m = sum(R[q][k] for q in ("egb", "evdw", "ecav", "ehb"))
         e_f = sum(F[q] for q in ("egb", "evdw", "ecav", "ehb"))
         acc.append(abs(e_m - e_f) / abs(e_f))
         a.close()
-    if rank == 0:
-        natoms = int(sum(x.natoms for x in systems))
-        print(json.dumps({
-            "metric": "instance energy+grad evals/s, 512-instance batch (300-5,000 atoms)", "value": value,
-            "unit": "evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": tot / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 math / f64 accumulation", "data": "synthetic",
-            "config": {"workload": f"batch of {args.ninst} globules, {natoms} atoms total, 0.2 A noise",
-                       "l2": "256 MB flush between timed steps", "autotune": tune},
-            "stage_ms": stage_ms,
-            "e2e": {"value": world * args.ninst * args.steps / sum(e2e), "unit": "evals/s",
-                    "h2d_bytes_per_step": 3 * 8 * natoms, "d2h_bytes_per_step": 15 * 8 * natoms + 56 * args.ninst},
-            "accuracy_vs_fp64": {"max_energy_rel_err": max(acc)},
-            "gpu_launches": launches * args.steps,
-            "clocks": clk.summary()}))
+    natoms = int(sum(x.natoms for x in systems))
     B.close()
     for i in insts:
         i.close()
+    return {"value": value, "unit": "evals/s", "ms_per_step": tot / steps, "steps": steps, "warmup": warmup,
+            "workload": f"batch of {ninst} globules, {natoms} atoms total, 0.2 A noise", "natoms": natoms,
+            "autotune": tune, "stage_ms": stage_ms,
+            "e2e": {"value": world * ninst * steps / sum(e2e), "unit": "evals/s",
+                    "h2d_bytes_per_step": 3 * 8 * natoms, "d2h_bytes_per_step": 15 * 8 * natoms + 56 * ninst},
+            "accuracy_vs_fp64": {"max_energy_rel_err": max(acc)}, "launches_per_step": launches,
+            "clocks": clk.summary() if clk else None}
+
+
+def batch_main(args, A, torch, rank, world, local):
+    """512 independent instances (log-uniform 300-5,000 atoms, 0.2 A noise)
+    evaluated together: one step = one batched evaluation of all instances;
+    the metric is instance evaluations per second."""
+    m = measure_batch(A, torch, args.ninst, args.steps, args.warmup, args.seed, rank, world, local)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "instance energy+grad evals/s, 512-instance batch (300-5,000 atoms)", "value": m["value"],
+            "unit": "evals/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 math / f64 accumulation", "data": "synthetic",
+            "config": {"workload": m["workload"], "l2": "256 MB flush between timed steps", "autotune": m["autotune"]},
+            "stage_ms": m["stage_ms"], "e2e": m["e2e"], "accuracy_vs_fp64": m["accuracy_vs_fp64"],
+            "gpu_launches": m["launches_per_step"] * args.steps, "clocks": m["clocks"]}))
 
 
 def shard_main(args, A, torch, rank, world, local):
@@ -488,24 +578,63 @@ def main():
     e2e_tot = max_over_ranks(sum(e2e_t), world, f"cuda:{local}")
     e2e_value = throughput(args.steps, e2e_tot, world)
 
+    # the same call with pageable host arrays (plain numpy), as a C caller
+    # passing its own malloc'd arrays would
+    pg = [np.ascontiguousarray(a, dtype=np.float64) for a in (s.x, s.y, s.z)]
+    pouts = [np.zeros(natoms) for _ in range(3)] + [np.zeros((natoms, 3)) for _ in range(4)]
+    pptr = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+
+    def call_pageable():
+        rc = L.agbnp3_ener(inst.tag, 0, pptr(pg[0]), pptr(pg[1]), pptr(pg[2]), pptr(pouts[0]), pptr(pouts[1]),
+                           ctypes.byref(es[6]), pptr(pouts[2]), ctypes.byref(es[0]), pptr(pouts[3]),
+                           ctypes.byref(es[1]), ctypes.byref(es[2]), pptr(pouts[4]), ctypes.byref(es[3]),
+                           ctypes.byref(es[4]), pptr(pouts[5]), ctypes.byref(es[5]), pptr(pouts[6]))
+        if rc != A.AGBNP_OK:
+            raise RuntimeError(A.last_error())
+
+    for _ in range(args.warmup):
+        call_pageable()
+    e2e_p = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        call_pageable()
+        e2e_p.append(time.perf_counter() - t0)
+    e2e_pageable = throughput(args.steps, max_over_ranks(sum(e2e_p), world, f"cuda:{local}"), world)
+
     # roofline of the pair stages: algorithmic FP32 work per launch (pair
     # counts x frozen per-pair operation counts) over the stage's device
     # time, against FP32 / special-function peaks measured in this run
     peaks = A.measure_peaks(local)
     roof = pair_roofline(natoms, s.nheavy, stage_ms, peaks)
+    hbm = measured_hbm_gbs()
+    roof["hbm_stages"] = tree_roofline(natoms, s.nheavy, st, stage_ms, hbm["gbs"], 4, load_traffic(natoms))
+    roof["hbm_stages_peak"] = hbm
+
+    # the batched configuration (512 instances), measured in the same run
+    batch = None
+    if not args.no_batch:
+        batch = measure_batch(A, torch, args.ninst, args.batch_steps, 3, args.seed, rank, world, local,
+                              clocks=False)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and os.path.exists(os.path.join(ROOT, "oracle", "_ref",
                                                                              "libagbnp3_ref.so")):
         try:
             threads = os.cpu_count() or 1
-            d = run_reference(natoms, args.seed, 1, 0, threads)
-            cpu = {"value": 1.0 / d["times"][0], "unit": UNIT, "cores": threads, "kind": "reference",
-                   "sample": f"1 evaluation of the {natoms}-atom globule, reference library, {threads} OpenMP threads"}
+            k = args.cpu_best_of
+            d = run_reference(natoms, args.seed, k, 1, threads)
+            cpu = {"value": 1.0 / min(d["times"]), "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"best of {k} evaluations (after 1 untimed) of the {natoms}-atom globule, reference "
+                             f"library, {threads} OpenMP threads",
+                   "times_s": d["times"]}
             if not args.no_single_core and threads > 1:
-                d1 = run_reference(natoms, args.seed, 1, 0, 1)
-                cpu["single_core"] = {"value": 1.0 / d1["times"][0], "unit": UNIT, "cores": 1,
-                                      "sample": f"1 evaluation of the {natoms}-atom globule, 1 thread"}
+                d1 = run_reference(natoms, args.seed, k, 0, 1)
+                cpu["single_core"] = {"value": 1.0 / min(d1["times"]), "unit": UNIT, "cores": 1,
+                                      "sample": f"best of {k} evaluations of the {natoms}-atom globule, 1 thread",
+                                      "times_s": d1["times"]}
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
@@ -514,7 +643,7 @@ def main():
             "metric": metric_name(natoms), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 math / f64 accumulation", "data": "synthetic",
-            "config": {"workload": f"globule {natoms} atoms ({s.nheavy} heavy), 0.05 heavy/A^3, seed {args.seed}",
+            "config": {"workload": workload_name(natoms, s.nheavy, args.seed),
                        "mode": "mixed", "compat": True, "l2": "256 MB flush between timed steps", "autotune": tune,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "fp64_plain": {"value": fp64_value, "unit": UNIT, "ms_per_step": sum(t64) / len(t64), "autotune": tune64,
@@ -523,9 +652,12 @@ def main():
             "stage_ms": stage_ms,
             "counts": st,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * natoms,
-                    "d2h_bytes_per_step": (3 + 12) * 8 * natoms + 7 * 8},
+                    "d2h_bytes_per_step": (3 + 12) * 8 * natoms + 7 * 8, "host_buffers": "pinned",
+                    "pageable": {"value": e2e_pageable, "unit": UNIT,
+                                 "host_buffers": "pageable (numpy arrays, as a C caller's malloc'd arrays)"}},
             "gpu_launches": int(st["launches"]) * args.steps,
             "roofline": roof,
+            "batch512": batch,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }

@@ -20,7 +20,13 @@ def bench():
 PEAKS = {"fp32_tflops": 72.0, "fp64_tflops": 36.0, "ex2_tops": 4.6, "nominal_sm_mhz": 1965.0}
 
 
-def test_pair_roofline_25k(bench):
+def test_pair_roofline_25k(bench, tmp_path, monkeypatch):
+    import json
+    tr = tmp_path / "traffic.json"
+    tr.write_text(json.dumps({"command": "ncu ...", "workload": "w", "evals": 2,
+                              "kernels": {"k_gbders_sym": {"dram_bytes_per_launch": 2.5e6, "dram_bytes_per_eval": 2.5e6,
+                                                           "launches_per_eval": 1, "us_per_launch": 700.0}}}))
+    monkeypatch.setattr(bench, "TRAFFIC_JSON", str(tr))
     n, nh = 25000, 12500
     stage = {"invb": 0.32, "agb": 0.44, "gbders": 0.74}
     r = bench.pair_roofline(n, nh, stage, PEAKS)
@@ -37,7 +43,7 @@ def test_pair_roofline_25k(bench):
     # the dominant (slowest) pair kernel carries the headline fraction and its captured traffic
     assert r["kernel"] == "k_gbders_sym" and r["frac"] == st["gbders"]["fp32_frac"]
     assert r["achieved"] == pytest.approx(r["frac"] * r["peak"])
-    assert r["traffic"] == bench.NCU_TRAFFIC_25K["k_gbders_sym"]
+    assert r["traffic"] == 2.5e6 and "ncu ..." in r["traffic_note"]
     tot = sum(st[k]["gflop_per_launch"] for k in stage)
     assert st["all_pair_stages"]["tflops"] == pytest.approx(tot / (sum(stage.values()) * 1e-3) / 1e3)
 
@@ -92,3 +98,44 @@ def test_ncu_launch_summary(tmp_path):
     assert kernel_key("void k_tree_ders<float, 3>(View)") == "k_tree_ders<float, 3>"
     assert cnt["k_tree_ders<float, 3>"] == 2 and tot["k_tree_ders<float, 3>"] == pytest.approx(80000.0)
     assert tot["k_prep"] == pytest.approx(6000.0) and tot["k_tree_ders<float, 4>"] == pytest.approx(1000.0)
+
+
+def test_tree_roofline(bench):
+    """HBM roofline of the O(N) stages: algorithmic bytes from the counts,
+    fraction of the HBM peak, and the captured DRAM bytes of the stage's
+    kernels when a traffic record is given."""
+    counts = {"near_pairs": 300000, "kept": [160000, 350000, 240000, 60000], "water_sites": 6000}
+    stage = {"nblist": 0.1, "volumes": 0.16, "ws": 0.1, "treeders": 0.12}
+    tr = {"kernels": {"k_nl_slab": {"dram_bytes_per_eval": 1e6}, "k_cell_fill": {"dram_bytes_per_eval": 2e5},
+                      "k_tree_ders<float, 2>": {"dram_bytes_per_eval": 3e6}}}
+    r = bench.tree_roofline(25000, 12500, counts, stage, 6500.0, 4, tr)
+    assert r["nblist"]["alg_bytes"] == 16 * 12500 + 8 * 300000 + 8 * 12500
+    rec = sum(k * (48 + 4 * m) for m, k in zip(range(2, 6), counts["kept"]))
+    assert r["treeders"]["alg_bytes"] == rec + 32 * 12500 + 96 * 25000
+    for k, e in r.items():
+        assert e["achieved_gbs"] == pytest.approx(e["alg_bytes"] / (stage[k] * 1e-3) / 1e9)
+        assert e["frac_of_hbm"] == pytest.approx(e["achieved_gbs"] / 6500.0)
+    assert r["nblist"]["dram_bytes_ncu"] == pytest.approx(1.2e6)
+    assert r["treeders"]["dram_bytes_ncu"] == pytest.approx(3e6)
+    assert r["ws"]["dram_bytes_ncu"] == 0
+
+
+def test_ncu_traffic_summary(tmp_path):
+    """DRAM bytes per launch and per evaluation from a capture with the
+    dram__bytes metrics (units converted)."""
+    from agbnp3_b200.ncu_summary import traffic
+    hdr = ('"ID","Process ID","Process Name","Host Name","Kernel Name","Context","Stream","Block Size","Grid Size",'
+           '"Device","CC","Section Name","Metric Name","Metric Unit","Metric Value"\n')
+    rows = []
+    for i in range(2):
+        rows += [(i, "k_agb_sym(View)", "gpu__time_duration.sum", "us", "450"),
+                 (i, "k_agb_sym(View)", "dram__bytes_read.sum", "Mbyte", "1.5"),
+                 (i, "k_agb_sym(View)", "dram__bytes_write.sum", "Kbyte", "500")]
+    text = hdr + "".join(f'"{i}","1","py","h","{k}","1","13","(128, 1, 1)","(1, 1, 1)","0","10.0","s","{m}","{u}","{v}"\n'
+                         for i, k, m, u, v in rows)
+    p = tmp_path / "cap.csv"
+    p.write_text(text)
+    t = traffic(str(p), evals=2)
+    assert t["k_agb_sym"]["dram_bytes_per_launch"] == pytest.approx(2.0e6)
+    assert t["k_agb_sym"]["dram_bytes_per_eval"] == pytest.approx(2.0e6)
+    assert t["k_agb_sym"]["us_per_launch"] == pytest.approx(450.0)
