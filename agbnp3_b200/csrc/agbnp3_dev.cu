@@ -64,6 +64,7 @@
 #define C_AMAX 20.0
 
 #define BLK 128
+#define FULLMASK 0xffffffffu
 
 struct __align__(16) f4 {
   float x, y, z, w;
@@ -92,9 +93,9 @@ struct View {
   f4 *cell_pos;  /* per bucket slot: the atom's position and radius */
   int2 *cell_id; /* per bucket slot: the atom and its packed cell */
   int *nl_count, *nl_off, *nl_list;
-  int slab_w;            /* near partners an atom's slab holds */
-  int *slab_j;           /* [natoms * slab_w] partners, unordered */
-  float *slab_d2;        /* [natoms * slab_w] their float d^2 */
+  int slab_w;            /* near partners an (atom, neighbour cell) sub-slab holds */
+  int *slab_j;           /* [natoms * 27 * slab_w] partners, unordered */
+  float *slab_d2;        /* [natoms * 27 * slab_w] their float d^2 */
   float *nl_d2;
   int cap_nl;
   int cap[AGB_MAX_ORDER + 1];
@@ -153,8 +154,9 @@ enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m
           (27 N when rebuilding, else 0), that scan's total, the live
           candidates of the last build, builds so far */
        DC_REBUILD = DC_C0 + 8, DC_CLEN, DC_CTOT, DC_NCAND, DC_NBUILD,
-       DC_SLABMAX /* near partners of the fullest overflowing slab */ };
-#define DC_SIZE (DC_C0 + 14)
+       DC_SLABMAX /* near partners of the fullest overflowing (atom, cell) sub-slab */,
+       DC_N27 /* 27 N */ };
+#define DC_SIZE (DC_C0 + 15)
 
 /* record fields of a kept overlap, stored contiguously per record (12
    slots, three 4-wide vectors) */
@@ -385,57 +387,80 @@ __device__ __forceinline__ void for_cell(const View &v, int I, int ax, int ay, i
   }
 }
 
-/* one thread per (heavy atom, neighbour cell): the atom's near partners
-   j > i go to its own slab of slab_w entries, in any order (the ranking
-   below fixes it), counted by an atomic per atom; an overflowing slab sets
-   the error word and the largest count needed */
-__global__ void k_nl_slab(View v) {
+/* one thread per (heavy atom, neighbour cell), taken direction-major over
+   the pair slots (a warp's atoms are spatially close and look into the
+   same neighbour direction): the atom's partners j > i in that cell that
+   pass the near test go to the (atom, cell) sub-slab of slab_w entries,
+   their number to nl_c27.  No atomics: every entry and count has one
+   writer.  An overflowing sub-slab sets the error word and the largest
+   count needed. */
+__global__ void k_nl_c27(View v) {
   AGB_GRID_STRIDE(q, 27LL * v.natoms) {
-    /* cell-major over the pair slots: the lanes of a warp hold spatially
-       close atoms looking into the same neighbour direction */
-    int c = (int)(q / v.natoms), g = v.slot_atom[(int)(q % v.natoms)];
-    int I = v.inst_of[g];
-    if (g >= v.inst_begin[I] + v.inst_nheavy[I]) continue;
-    f4 a = v.pos[g];
-    const size_t base = (size_t)g * v.slab_w;
-    for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
-             v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j, const f4 &b) {
-               float d2;
-               if (j > g && near_test(a, b, d2)) {
-                 int k = atomicAdd(&v.nl_count[g], 1);
-                 if (k < v.slab_w) {
-                   v.slab_j[base + k] = j;
-                   v.slab_d2[base + k] = d2;
-                 } else {
-                   set_err(v, AGB_ERR_NL_CAP);
-                   atomicMax(&v.dc[DC_SLABMAX], k + 1);
+    const int c = (int)(q / v.natoms), g = v.slot_atom[(int)(q % v.natoms)];
+    const int I = v.inst_of[g];
+    int cnt = 0;
+    if (g < v.inst_begin[I] + v.inst_nheavy[I]) {
+      const f4 a = v.pos[g];
+      const size_t base = ((size_t)g * 27 + c) * v.slab_w;
+      for_cell(v, I, v.atom_cell[3 * g] + c % 3 - 1, v.atom_cell[3 * g + 1] + (c / 3) % 3 - 1,
+               v.atom_cell[3 * g + 2] + c / 9 - 1, [&](int j, const f4 &b) {
+                 float d2;
+                 if (j > g && near_test(a, b, d2)) {
+                   if (cnt < v.slab_w) {
+                     v.slab_j[base + cnt] = j;
+                     v.slab_d2[base + cnt] = d2;
+                   }
+                   cnt++;
                  }
-               }
-             });
+               });
+      if (cnt > v.slab_w) {
+        set_err(v, AGB_ERR_NL_CAP);
+        atomicMax(&v.dc[DC_SLABMAX], cnt); /* capacity statistic of the error path */
+      }
+    }
+    v.nl_c27[27 * g + c] = cnt;
   }
 }
 
 /* each atom's list in (float d^2, index) order (agbnp3.c:3766-3792,
-   4062-4066): one warp per atom, each slab entry placed at its rank */
-__global__ void k_nl_slab_rank(View v) {
+   4062-4066), one warp per atom: lane c < 27 copies its cell's sub-slab to
+   the atom's range of the list (placed by the scan of the per-cell
+   counts), then every entry is written at its rank */
+__global__ void k_nl_rank27(View v) {
   if (v.dc[DC_ERR] & AGB_ERR_NL_CAP) return;
   const int lane = threadIdx.x & 31;
   const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long g = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < v.natoms; g += nw) {
-    const int m = v.nl_count[g], o = v.nl_off[g];
+    const int cnt = lane < 27 ? v.nl_c27[27 * g + lane] : 0;
+    int x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULLMASK, x, o);
+      if (lane >= o) x += y;
+    }
+    const int m = __shfl_sync(FULLMASK, x, 31), o = v.nl_o27[27 * g];
+    if (lane == 0) {
+      v.nl_off[g] = o;
+      v.nl_count[g] = m;
+    }
     if (m == 0) continue;
     if (o + m > v.cap_nl) {
       if (lane == 0) set_err(v, AGB_ERR_NL_CAP);
       continue;
     }
-    const size_t base = (size_t)g * v.slab_w;
+    const size_t sb = ((size_t)g * 27 + lane) * v.slab_w;
+    for (int k = 0; k < cnt; k++) {
+      v.nl_tmp[o + x - cnt + k] = v.slab_j[sb + k];
+      v.nl_d2[o + x - cnt + k] = v.slab_d2[sb + k];
+    }
+    __syncwarp();
     for (int k = lane; k < m; k += 32) {
-      const float d2 = v.slab_d2[base + k];
-      const int j = v.slab_j[base + k];
+      const float d2 = v.nl_d2[o + k];
+      const int j = v.nl_tmp[o + k];
       int rank = 0;
       for (int b = 0; b < m; b++) {
-        float db = v.slab_d2[base + b];
-        rank += (db < d2) || (db == d2 && v.slab_j[base + b] < j);
+        const float db = v.nl_d2[o + b];
+        rank += (db < d2) || (db == d2 && v.nl_tmp[o + b] < j);
       }
       v.nl_list[o + rank] = j;
       v.nl_own[o + rank] = (int)g;
@@ -1372,7 +1397,6 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
 /* Partial sums are in the working precision over a j tile (j side) or a    */
 /* j run (i side), then double.                                              */
 /* ------------------------------------------------------------------------ */
-#define FULLMASK 0xffffffffu
 
 template <typename T>
 __device__ __forceinline__ T rot1(T x) {
@@ -2465,8 +2489,8 @@ static int tree_alloc(agb_dev *s) {
   CK(cudaMalloc((void **)&s->v.nl_own, sizeof(int) * (size_t)s->cap_nl));
   s->v.slab_w = 0;
   if (s->v.skin <= 0.0f) { /* the slabs of the per-evaluation search */
-    CK(cudaMalloc((void **)&s->v.slab_j, sizeof(int) * (size_t)s->natoms * s->slab_w));
-    CK(cudaMalloc((void **)&s->v.slab_d2, sizeof(float) * (size_t)s->natoms * s->slab_w));
+    CK(cudaMalloc((void **)&s->v.slab_j, sizeof(int) * (size_t)s->natoms * 27 * s->slab_w));
+    CK(cudaMalloc((void **)&s->v.slab_d2, sizeof(float) * (size_t)s->natoms * 27 * s->slab_w));
     s->v.slab_w = s->slab_w;
   }
   int maxcap = s->natoms;
@@ -2865,6 +2889,7 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   int dc0[DC_SIZE];
   memset(dc0, 0, sizeof(dc0));
   dc0[DC_N] = N;
+  dc0[DC_N27] = 27 * N;
   dc0[DC_NB] = nb;
   dc0[DC_NWS] = NW;
   dc0[DC_W27] = 27 * NW;
@@ -2879,7 +2904,7 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   s->cap[4] = 64 * nheavy_tot + 4096;
   s->cap[5] = 32 * nheavy_tot + 4096;
   s->cap_wsc = 64 * NW + 1024;
-  s->slab_w = 96; /* ~29 near partners j > i per heavy atom on average */
+  s->slab_w = 8; /* ~29 near partners j > i per heavy atom on average, over 27 cells */
   /* AGBNP3_CAPACITY_SCALE (< 1) starts from smaller buffers, which
      exercises the overflow detection and regrowth of agb_dev_evaluate */
   const char *cs = getenv("AGBNP3_CAPACITY_SCALE");
@@ -3194,11 +3219,10 @@ static void launch_all(agb_dev *s, int seg = -1) {
     AGB_LAUNCH(k_nl_rank, nblocks(s->cap_nl), BLK, st, v);
     nl += 9 + 2 * AGB_SCAN_LAUNCHES;
   } else {
-    cudaMemsetAsync(v.nl_count, 0, sizeof(int) * N, st);
     cudaMemsetAsync(v.dc + DC_SLABMAX, 0, sizeof(int), st);
-    AGB_LAUNCH(k_nl_slab, nblocks(27LL * N), BLK, st, v);
-    agb_scan_excl(v.nl_count, v.nl_off, v.dc + DC_N, v.dc + DC_NL, N, s->scan_scratch, st);
-    AGB_LAUNCH(k_nl_slab_rank, nblocks(32LL * N), BLK, st, v);
+    AGB_LAUNCH(k_nl_c27, nblocks(27LL * N), BLK, st, v);
+    agb_scan_excl(v.nl_c27, v.nl_o27, v.dc + DC_N27, v.dc + DC_NL, 27 * N, s->scan_scratch, st);
+    AGB_LAUNCH(k_nl_rank27, nblocks(32LL * N), BLK, st, v);
     nl += 2 + AGB_SCAN_LAUNCHES;
   }
   nl += 2 + AGB_SCAN_LAUNCHES; /* cell grid */
@@ -3382,7 +3406,7 @@ extern "C" int agb_dev_evaluate(agb_dev *s) {
     if (err & (AGB_ERR_NL_CAP | AGB_ERR_TREE_CAP | AGB_ERR_WS_CAP | AGB_ERR_CAND_CAP)) {
       /* grow what overflowed and evaluate again */
       if (dc[DC_NL] > s->cap_nl) s->cap_nl = 2 * dc[DC_NL];
-      if (dc[DC_SLABMAX] > s->slab_w) s->slab_w = dc[DC_SLABMAX] + 32;
+      if (dc[DC_SLABMAX] > s->slab_w) s->slab_w = dc[DC_SLABMAX] + 4;
       if ((err & AGB_ERR_CAND_CAP) && dc[DC_CTOT] > s->cap_cand) s->cap_cand = 2 * dc[DC_CTOT];
       if (dc[DC_WSC] > s->cap_wsc) s->cap_wsc = 2 * dc[DC_WSC];
       for (int m = 2; m <= AGB_MAX_ORDER; m++)

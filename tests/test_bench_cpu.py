@@ -24,7 +24,7 @@ def test_pair_roofline_25k(bench, tmp_path, monkeypatch):
     import json
     tr = tmp_path / "traffic.json"
     tr.write_text(json.dumps({"command": "ncu ...", "workload": "w", "evals": 2,
-                              "kernels": {"k_gbders_sym": {"dram_bytes_per_launch": 2.5e6, "dram_bytes_per_eval": 2.5e6,
+                              "kernels": {"k_gbders_x2<1>": {"dram_bytes_per_launch": 2.5e6, "dram_bytes_per_eval": 2.5e6,
                                                            "launches_per_eval": 1, "us_per_launch": 700.0}}}))
     monkeypatch.setattr(bench, "TRAFFIC_JSON", str(tr))
     n, nh = 25000, 12500
@@ -41,7 +41,7 @@ def test_pair_roofline_25k(bench, tmp_path, monkeypatch):
     for k, ms in stage.items():
         assert st[k]["fp32_frac"] == pytest.approx(st[k]["gflop_per_launch"] / (ms * 1e-3) / 1e3 / PEAKS["fp32_tflops"])
     # the dominant (slowest) pair kernel carries the headline fraction and its captured traffic
-    assert r["kernel"] == "k_gbders_sym" and r["frac"] == st["gbders"]["fp32_frac"]
+    assert r["kernel"] == "k_gbders_x2" and r["frac"] == st["gbders"]["fp32_frac"]
     assert r["achieved"] == pytest.approx(r["frac"] * r["peak"])
     assert r["traffic"] == 2.5e6 and "ncu ..." in r["traffic_note"]
     tot = sum(st[k]["gflop_per_launch"] for k in stage)
@@ -50,7 +50,7 @@ def test_pair_roofline_25k(bench, tmp_path, monkeypatch):
 
 def test_pair_roofline_other_size_has_no_traffic(bench):
     r = bench.pair_roofline(100000, 50000, {"invb": 4.0, "agb": 6.7, "gbders": 7.6}, PEAKS)
-    assert r["kernel"] == "k_gbders_sym" and r["traffic"] is None
+    assert r["kernel"] == "k_gbders_x2" and r["traffic"] is None
     assert 0.0 < r["frac"] < 1.5
 
 
