@@ -93,6 +93,7 @@ def lib():
         L.agbnp3_batch_natoms.argtypes = [ctypes.c_int]
         L.agbnp3_batch_set_coords.argtypes = [ctypes.c_int, _dp, _dp, _dp]
         L.agbnp3_batch_ener_resident.argtypes = [ctypes.c_int]
+        L.agbnp3_batches_ener_resident.argtypes = [ctypes.c_int, _ip]
         L.agbnp3_batch_get_results.argtypes = [ctypes.c_int] + [_dp] * 8
         L.agbnp3_batch_set_mode.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.agbnp3_batch_stream.argtypes = [ctypes.c_int]
@@ -435,3 +436,10 @@ class Batch:
         if self.btag is not None:
             lib().agbnp3_batch_delete(self.btag)
             self.btag = None
+
+
+def ener_resident_many(batches):
+    """Evaluates several distinct batches at once (agbnp3_batches_ener_resident):
+    their captured evaluations run side by side, each on its own stream."""
+    tags = np.array([b.btag for b in batches], dtype=np.int32)
+    _check(lib().agbnp3_batches_ener_resident(len(tags), _p(tags, _ip)), "agbnp3_batches_ener_resident")

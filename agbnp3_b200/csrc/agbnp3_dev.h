@@ -88,6 +88,9 @@ int agb_dev_upload_coords(agb_dev *s, const double *x, const double *y, const do
    the device.  Returns 0, or a negative error after checking the device
    error word (capacities are grown and the evaluation repeated on overflow). */
 int agb_dev_evaluate(agb_dev *s);
+/* several independent evaluations (distinct objects) issued together, each
+   on its own stream, then checked one by one */
+int agb_dev_evaluate_many(agb_dev *const *ss, int n);
 /* pair-stage slot order: 1 = along a Hilbert curve (set from the
    coordinates of the next evaluation), 0 = identity */
 int agb_dev_set_pair_order(agb_dev *s, int mode);

@@ -1022,6 +1022,29 @@ int agbnp3_batch_ener_resident(int btag) {
   return B ? eval_dev(B->dev, "agbnp3_batch_ener_resident()") : AGBNP_ERR;
 }
 
+int agbnp3_batches_ener_resident(int nb, const int *btags) {
+  agb_dev *devs[64];
+  if (nb <= 0 || nb > 64 || !btags) {
+    errprint("agbnp3_batches_ener_resident(): %d batches (1 to 64).", nb);
+    return AGBNP_ERR;
+  }
+  for (int k = 0; k < nb; k++) {
+    batch_t *B = get_batch(btags[k], "agbnp3_batches_ener_resident()");
+    if (!B) return AGBNP_ERR;
+    for (int q = 0; q < k; q++)
+      if (btags[q] == btags[k]) {
+        errprint("agbnp3_batches_ener_resident(): batch %d given twice.", btags[k]);
+        return AGBNP_ERR;
+      }
+    devs[k] = B->dev;
+  }
+  if (agb_dev_evaluate_many(devs, nb) != 0) {
+    errprint("agbnp3_batches_ener_resident(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  return AGBNP_OK;
+}
+
 int agbnp3_batch_get_results(int btag, double *energies, double *sp, double *br, double *surf_area,
                              double (*dgbdr)[3], double (*dvwdr)[3], double (*decav)[3], double (*dehb)[3]) {
   batch_t *B = get_batch(btag, "agbnp3_batch_get_results()");

@@ -21,7 +21,7 @@ __global__ void k_scan_tiles(const int *__restrict__ in, const int *__restrict__
     int s = 0;
     for (int k = 0; k < SCAN_ITEMS; k++) {
       long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
-      if (i < len) s += in[i];
+      if (i < len) s += max(in[i], 0); /* counts are never negative */
     }
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
@@ -77,7 +77,7 @@ __global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, 
     int s = 0;
     for (int k = 0; k < SCAN_ITEMS; k++) {
       long long i = base + (long long)threadIdx.x * SCAN_ITEMS + k;
-      v[k] = i < len ? in[i] : 0;
+      v[k] = i < len ? max(in[i], 0) : 0; /* counts are never negative */
       s += v[k];
     }
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -104,7 +104,7 @@ __global__ void k_scan_apply(const int *__restrict__ in, int *__restrict__ out, 
         out[i] = run;
         /* the item each output slot belongs to (bounded by owner_cap) */
         if (owner)
-          for (int t = 0; t < v[k] && run + t < owner_cap; t++) owner[run + t] = (int)i;
+          for (int t = max(0, -run); t < v[k] && run + t < owner_cap; t++) owner[run + t] = (int)i;
       }
       run += v[k];
     }

@@ -11,6 +11,7 @@ one of its kernels (agbnp3_mlp_*).  torch only holds the device buffers.
 
     python -m agbnp3_b200.surrogate train --out model.npz [--conformations 2000 --natoms 5000]
     python -m agbnp3_b200.surrogate evaluate --model model.npz --natoms 25000
+    python -m agbnp3_b200.surrogate bound [--natoms N]   (accuracy the sums need)
 
 Training data: perturbed conformations (N(0, 0.3 A) coordinate noise) of
 seeded globules, labelled by the plain FP64 path of the engine.
@@ -27,6 +28,7 @@ from . import AGBNP_OK, AGBNPError, Instance, PREC_FP64, last_error, lib, make_g
 NIN, NH, NOUT = 160, 128, 2
 CLASS_RADII = (1.7, 1.55, 1.52, 1.8, 1.15)  # C, N, O, S, H (A, without the 0.5 A increment)
 ATOM_DESC_SUM, ATOM_SP = 19, 3  # per-atom debug arrays: descreening sum, sp
+ATOM_Q2AB, ATOM_ABRW = 12, 13  # the chain-rule factors through the Born radii
 
 
 def _bind():
@@ -285,6 +287,33 @@ def born_radii(S, radius):
     return 1.0 / bf
 
 
+def sum_accuracy_bound(S, radius, q2ab, abrw, e_total, eps_in, eps_out, target=1e-4):
+    """How accurately a surrogate must reproduce the descreening sums S_i
+    (the sum in 1/B_i = 1/R_i - S_i/4pi) for the total energy to stay within
+    `target` (relative), to first order.
+
+    dE/dS_i = -(332 df q2ab_i + abrw_i) / 4pi with df = -(1/eps_in -
+    1/eps_out)/2: the GB energy and the vdW term depend on S_i only through
+    B_i (agbnp3_utils.c:615-670, agbnp3.c:1466-1487; q2ab_i and abrw_i are
+    the chain-rule factors the engine forms after the GB pair pass,
+    agbnp3_cpu_simd_kernels.c:440-457).  With w_i = S_i dE/dS_i, relative
+    errors e_i of the sums move the energy by sum_i w_i e_i: independent
+    errors of RMS sigma by sigma |w|_2 (RMS), a common relative error sigma
+    by sigma |sum_i w_i|.  Returns the largest sigma of each kind, and the
+    distribution of kappa_i = (S_i/4pi) / beta_i, the factor by which the
+    subtraction 1/R_i - S_i/4pi amplifies a relative error of S_i."""
+    S, radius, q2ab, abrw = (np.asarray(a, dtype=np.float64) for a in (S, radius, q2ab, abrw))
+    df = -0.5 * (1.0 / eps_in - 1.0 / eps_out)
+    w = -(332.0 * df * q2ab + abrw) * S / (4.0 * np.pi)
+    beta = 1.0 / radius - S / (4.0 * np.pi)
+    kappa = (S / (4.0 * np.pi)) / np.maximum(beta, 1e-12)
+    return {"target": target,
+            "sigma_random": float(target * abs(e_total) / np.sqrt((w ** 2).sum())),
+            "sigma_common": float(target * abs(e_total) / abs(w.sum())),
+            "kappa_median": float(np.median(kappa)), "kappa_p90": float(np.percentile(kappa, 90)),
+            "kappa_max": float(kappa.max())}
+
+
 # largest system agbnp3_gb_energy_static accepts (the size of its static
 # device scratch array)
 STATIC_MAX_ATOMS = 32768
@@ -316,19 +345,25 @@ def gb_energy(system, int2ext, radii_b):
 
 
 def gain(models, natoms, seed=1, tolerances=(0.0, 0.01, 0.03, 0.1, 0.3, float("inf"))):
-    """What the ensemble surrogate gains on one globule: for each tolerance of
-    the residual check (atoms whose two networks disagree by more than tol on
-    the descreening sum fall back to the exact sum), the fraction that falls
-    back, the relative error of the GB energy, and the modelled time of the
-    descreening stage (surrogate + the fallback's share of the exact stage)
-    against the exact stage alone."""
+    """What the ensemble surrogate gains on one globule, all measured:
+    - the device time of the surrogate inference (features + networks) and of
+      the exact descreening stage it would replace (chosen mode);
+    - for each tolerance of the residual check (atoms whose two networks
+      disagree by more than tol on the descreening sum fall back to the
+      exact sum) the fraction that falls back and the relative error of the
+      GB energy at the resulting Born radii;
+    - the networks' relative RMS error of the sums against the accuracy the
+      1e-4 energy target needs (sum_accuracy_bound, from the FP64 path's
+      chain-rule factors)."""
     from . import PREC_MIXED
     s = make_globule(natoms, seed)
     int2ext, _ = s.internal_order()
     radius = np.asarray(s.r)[int2ext]
     inst = Instance(s, precision=PREC_FP64)
-    inst.ener()
+    R64 = inst.ener()
     exact = labels(inst, natoms, s)[:, 0]
+    bound = sum_accuracy_bound(exact, radius, inst.atom_array(ATOM_Q2AB), inst.atom_array(ATOM_ABRW),
+                               sum(R64[k] for k in ("egb", "evdw", "ecav", "ehb")), s.eps_in, s.eps_out)
     # the exact stage's time, from the chosen (mixed) path
     mixed = Instance(s, precision=PREC_MIXED)
     mixed.ener()
@@ -373,15 +408,18 @@ def gain(models, natoms, seed=1, tolerances=(0.0, 0.01, 0.03, 0.1, 0.3, float("i
         e = gb_energy(s, int2ext, born_radii(S, radius))
         frac = float(fall.mean())
         rows.append({"tolerance": tol, "fallback_fraction": frac, "egb_rel_err": abs(e - e_exact) / abs(e_exact),
-                     "modelled_ms": t_sur + frac * t_exact, "exact_ms": t_exact,
                      "rms_sum_err": float(np.sqrt(((S - exact) ** 2).mean()))})
     inst.close()
-    return {"natoms": natoms, "surrogate_ms": t_sur, "exact_stage_ms": t_exact, "egb": e_exact, "rows": rows}
+    ok = [q["fallback_fraction"] for q in rows if q["egb_rel_err"] <= 1e-4]
+    return {"natoms": natoms, "surrogate_ms": t_sur, "exact_stage_ms": t_exact,
+            "stage_speedup_without_fallback": t_exact / t_sur, "egb": e_exact, "rows": rows,
+            "network_rel_rms_err": float(np.sqrt((((mean - exact) / np.abs(exact)) ** 2).mean())),
+            "accuracy_bound": bound, "min_fallback_meeting_1e-4": min(ok) if ok else None}
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["train", "evaluate", "gain"])
+    ap.add_argument("cmd", choices=["train", "evaluate", "gain", "bound"])
     ap.add_argument("--models", nargs="*", default=[])
     ap.add_argument("--seeds", type=int, nargs="*", default=[0])
     ap.add_argument("--out", default="surrogate_model.npz")
@@ -400,6 +438,18 @@ def main():
             out = a.out.replace("{seed}", str(sd))
             np.savez(out, **model)
             print(f"saved {out}")
+    elif a.cmd == "bound":
+        import json
+        for n in (a.natoms,) if a.natoms != 5000 else (5000, 25000, 50000):
+            s = make_globule(n, 1)
+            inst = Instance(s, precision=PREC_FP64)
+            R = inst.ener()
+            int2ext, _ = s.internal_order()
+            b = sum_accuracy_bound(inst.atom_array(ATOM_DESC_SUM), np.asarray(s.r)[int2ext],
+                                   inst.atom_array(ATOM_Q2AB), inst.atom_array(ATOM_ABRW),
+                                   sum(R[k] for k in ("egb", "evdw", "ecav", "ehb")), s.eps_in, s.eps_out)
+            print(json.dumps({"natoms": n, **b}))
+            inst.close()
     elif a.cmd == "gain":
         import json
         r = gain([dict(np.load(m)) for m in a.models], a.natoms)

@@ -140,6 +140,12 @@ int agbnp3_batch_delete(int btag);
 int agbnp3_batch_natoms(int btag);
 int agbnp3_batch_set_coords(int btag, const double *x, const double *y, const double *z);
 int agbnp3_batch_ener_resident(int btag);
+/* agbnp3_batch_ener_resident of nb distinct batches (1..64) at once: each
+   batch's captured evaluation is launched on its own stream before any is
+   waited for, so one batch's latency-bound stages (near list, overlap tree,
+   water sites, tree derivatives) run beside another's pair passes.  Returns
+   when all are done; results as after agbnp3_batch_ener_resident. */
+int agbnp3_batches_ener_resident(int nb, const int *btags);
 /* energies: [ntags][7] as in agbnp3_get_results */
 int agbnp3_batch_get_results(int btag, double *energies, double *sp, double *br, double *surf_area,
                              double (*dgbdr)[3], double (*dvwdr)[3], double (*decav)[3], double (*dehb)[3]);

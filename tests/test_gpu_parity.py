@@ -407,6 +407,29 @@ def test_capacity_regrowth(engine, monkeypatch):
 
 
 @pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+def test_regrowth_on_reused_device_memory(engine, monkeypatch, prec):
+    """A first evaluation whose near-list sub-slabs and overlap buffers
+    overflow, on device memory that held other data before (1 GB of -7
+    written and handed back to the driver): the passes that run after the
+    overflow was flagged must not take counts from what the memory held,
+    and the repeated evaluation gives the oracle's results."""
+    import torch
+    junk = torch.full((256 * 1024 * 1024,), -7, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    del junk
+    torch.cuda.empty_cache()
+    s = A.make_globule(2500, 21, noise=0.2)
+    q = O.oracle_eval(s)
+    monkeypatch.setenv("AGBNP3_CAPACITY_SCALE", "0.01")
+    inst = A.Instance(s, precision=prec)
+    try:
+        check_vs_oracle(inst.ener(), q, prec, "regrowth on reused memory")
+        assert inst.stats()["error"] == 0
+    finally:
+        inst.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
 def test_one_sided_pair_kernels(engine, monkeypatch, prec):
     """The one-sided tiled GB pair kernels (AGBNP3_PAIR_TILED=1, each
     ordered pair evaluated by its first atom) against the oracle, and in
@@ -466,3 +489,63 @@ def test_pair_slot_order(engine, prec):
         check_vs_oracle(r2, O.oracle_eval(s2), prec, "reordered")
     finally:
         inst.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+def test_descreening_range_culling(engine, prec):
+    """A 3,000-atom globule spread to three times its size (most atom pairs
+    lie beyond the Q4 tables' range, so the descreening pass skips most
+    partner tiles by their bounding boxes): Born radii, energies and forces
+    still equal the FP64 oracle's at the single-instance tolerances.  The
+    spread water sites overlap nothing, so the HB gradient is ~1e-15 and is
+    compared within the sum of all four gradients."""
+    s0 = A.make_globule(3000, 11)
+    s = s0.with_coords(3.0 * s0.coords())
+    Q = O.oracle_eval(s, compat=True)
+    inst = A.Instance(s, precision=prec)
+    t = TOL[prec]
+    try:
+        R = inst.ener()
+        for k in ENERGY_KEYS:
+            assert abs(R[k] - Q[k]) <= t["e"] * max(abs(Q[k]), 10.0), (k, R[k], Q[k])
+        for k in ("sp", "br", "surf_area", "dgbdr", "dvwdr", "decav"):
+            assert rms_rel(R[k], Q[k]) <= t["g"], (k, rms_rel(R[k], Q[k]))
+        tot = lambda X: X["dgbdr"] + X["dvwdr"] + X["decav"] + X["dehb"]  # noqa: E731
+        assert rms_rel(tot(R), tot(Q)) <= t["g"]
+    finally:
+        inst.close()
+
+
+def test_batches_side_by_side(engine):
+    """agbnp3_batches_ener_resident: three batches launched together on
+    their own streams give each batch's results from its own evaluation
+    (the same kernels on the same data; summation order of the double
+    atomics aside), on the first call (graphs captured one by one) and on
+    replays (graphs launched side by side)."""
+    groups = [[A.make_globule(n, 70 + 10 * q + k, noise=0.2) for k, n in enumerate(ns)]
+              for q, ns in enumerate(((400, 1300), (2500,), (600, 350, 900)))]
+    insts = [[A.Instance(x, precision=A.PREC_MIXED) for x in g] for g in groups]
+    alone = [A.Batch(m) for m in insts]
+    many = [A.Batch(m) for m in insts]
+    try:
+        for b, g in zip(alone + many, groups + groups):
+            b.set_mode(A.PREC_MIXED, True)
+            b.set_coords(np.concatenate([x.coords() for x in g]))
+        for b in alone:
+            b.ener_resident()
+        for rep in range(3):
+            A.ener_resident_many(many)
+            for b, c in zip(alone, many):
+                Ra, Rc = b.results(), c.results()
+                for e in ENERGY_KEYS:
+                    assert np.allclose(Rc[e], Ra[e], rtol=1e-12, atol=1e-12), (rep, e)
+                for g in ("sp", "br", "surf_area", "dgbdr", "dvwdr", "decav", "dehb"):
+                    assert rms_rel(Rc[g], Ra[g]) < 1e-12, (rep, g)
+        with pytest.raises(A.AGBNPError):
+            A.ener_resident_many([many[0], many[0]])
+    finally:
+        for b in alone + many:
+            b.close()
+        for m in insts:
+            for i in m:
+                i.close()
