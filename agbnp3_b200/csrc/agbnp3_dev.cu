@@ -1082,22 +1082,6 @@ struct alignas(2 * sizeof(R)) PartW {
 
 /* one staged group of partners against a thread's two atoms; SELF: the
    group may hold the atoms themselves (skipped) */
-/* interval index and fraction of a table coordinate 0 <= x < AGB_NA - 1.
-   In float without float->int conversions, which share the
-   special-function unit with the pass's square root: 2^23 + x rounded
-   toward minus infinity is 2^23 + floor(x), whose bit pattern is
-   0x4B000000 + floor(x); the fraction is exact either way */
-__device__ __forceinline__ int q4_split(float x, float &t) {
-  const float fk = __fadd_rd(x, 8388608.f);
-  t = x - (fk - 8388608.f);
-  return __float_as_int(fk) - 0x4B000000;
-}
-__device__ __forceinline__ int q4_split(double x, double &t) {
-  const int k = (int)x;
-  t = x - double(k);
-  return k;
-}
-
 template <typename R, bool SELF>
 __device__ __forceinline__ void desc_group(const Part4<R> *sp4, const PartW<R> *spw, int t0, int t1, int j0,
                                            const int (&g)[2], const R (&xg)[2], const R (&yg)[2], const R (&zg)[2],
@@ -1111,8 +1095,8 @@ __device__ __forceinline__ void desc_group(const Part4<R> *sp4, const PartW<R> *
       R dx = a.x - xg[u], dy = a.y - yg[u], dz = a.z - zg[u];
       R xh = p_sqrt(dx * dx + dy * dy + dz * dz) * a.rh;
       if (xh < R(AGB_NA - 1) && (!SELF || j0 + t != g[u])) {
-        R tt;
-        const int k = q4_split(xh, tt);
+        const int k = (int)xh;
+        R tt = xh - R(k);
         typename Tab<R>::T c = Tab<R>::ld(rowp[u] + b.t + k);
         part[u] += b.w * (c.x + tt * (c.y + tt * (c.z + tt * c.w)));
       }

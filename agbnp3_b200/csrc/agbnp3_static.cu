@@ -152,7 +152,9 @@ extern "C" int agbnp3_gb_energy_static(int natoms, const double *x, const double
     return st_fail("agbnp3_gb_energy_static(): no usable current device (%s)", cudaGetErrorString(e));
   if (!st_addr[dev]) {
     /* the array's name is a host-side stand-in; its device address comes
-       from the runtime, per device, with that device current */
+       from the runtime, per device, with that device current.  Two host
+       threads making their first call on one device at the same time both
+       store the same address here, so that race is harmless. */
     void *p = NULL;
     e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess || !p)
