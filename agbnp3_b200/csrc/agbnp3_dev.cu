@@ -2523,7 +2523,6 @@ struct agb_dev {
   int scalar_pairs; /* FP32: the scalar symmetric pair kernels instead of the packed f32x2 ones */
   int jb;          /* j tiles per symmetric work item */
   int items_prec;  /* precision the symmetric items were built for (i block size) */
-  int sfeat_ready; /* the feature kernel's shared-memory limit is set */
   int *h_inst_nheavy;
   int *h_ext_of;  /* external index of each internal atom */
   /* row sharding of one instance over ranks (one GPU each): this rank's
@@ -3957,48 +3956,104 @@ __device__ __forceinline__ void sf_add(float *row, int c, float d) {
   }
 }
 
+/* sf_add into a row shared by the lanes of a warp (shared-memory atomics) */
+__device__ __forceinline__ void sf_add_shared(float *row, int c, float d) {
+  const float delta = SF_RC / (SF_NB - 1), inv2s2 = 0.5f / (delta * delta);
+  const float fc = 0.5f * (__cosf(3.14159265358979f * d / SF_RC) + 1.f);
+  const int kc = __float2int_rn(d / delta);
+  const int k0 = max(0, kc - SF_W), k1 = min(SF_NB - 1, kc + SF_W);
+  for (int k = k0; k <= k1; k++) {
+    float u = d - (float)k * delta;
+    atomicAdd(&row[c * SF_NB + k], fc * __expf(-u * u * inv2s2));
+  }
+}
+
 /* features of every atom: for each neighbour class, the basis sum over the
    atoms of that class within SF_RC, plus the atom's own class at d = 0.  One
-   thread per atom scans the 27 grid cells around its own; its row of sums
-   lives in shared memory (stride SF_NF + 1).  Output: bf16
+   warp per atom.  Its lanes test the slots of the 27 grid cells around the
+   atom 32 at a time and append the neighbours within SF_RC (distance,
+   class) to a per-warp list in shared memory; every time the list holds 32,
+   each lane takes one and adds its basis terms to the warp's row of sums
+   (shared-memory atomics), so the basis work runs on full warps whatever
+   the share of candidates in range (about 1 in 6).  Output: bf16
    [natoms][SF_NF], internal order, each feature (x - mean) * invstd when
    mean / invstd are given. */
-#define SF_BLOCK 64
-__global__ void __launch_bounds__(SF_BLOCK) k_sfeat(View v, const float *__restrict__ mean,
-                                                    const float *__restrict__ invstd, __nv_bfloat16 *__restrict__ out) {
-  extern __shared__ float sacc[];
-  float *row = sacc + (size_t)threadIdx.x * (SF_NF + 1);
+#define SF_WARPS 4
+__global__ void __launch_bounds__(32 * SF_WARPS) k_sfeat(View v, const float *__restrict__ mean,
+                                                         const float *__restrict__ invstd,
+                                                         __nv_bfloat16 *__restrict__ out) {
+  __shared__ float srow[SF_WARPS][SF_NF];
+  __shared__ float sdist[SF_WARPS][64];
+  __shared__ int scls[SF_WARPS][64];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  float *row = srow[wp];
+  float *bd = sdist[wp];
+  int *bc = scls[wp];
   const float rc2 = SF_RC * SF_RC;
-  for (long long base = (long long)blockIdx.x * SF_BLOCK; base < v.natoms; base += (long long)gridDim.x * SF_BLOCK) {
-    const int g = (int)base + threadIdx.x;
-    if (g < v.natoms) {
-      for (int f = 0; f < SF_NF; f++) row[f] = 0.f;
-      const int I = v.inst_of[g];
-      const f4 pi = v.pos[g];
-      const int ci = v.sclass[g];
-      if (ci >= 0) sf_add(row, ci, 0.f);
-      int cx, cy, cz;
-      cell_of(pi.x, pi.y, pi.z, 1.0f / SF_RC, cx, cy, cz);
-      for (int c = 0; c < 27; c++) {
-        const int ax = cx + c % 3 - 1, ay = cy + (c / 3) % 3 - 1, az = cz + c / 9 - 1;
-        const int b = v.sf_bbegin[I] + cell_hash(ax, ay, az, v.sf_bmask[I]);
-        const int key = sf_key(ax, ay, az);
-        const int s0 = v.sf_bstart[b], s1 = s0 + v.sf_bcount[b];
-        for (int q = s0; q < s1; q++) {
+  const long long nw = (long long)gridDim.x * SF_WARPS;
+  for (long long gg = (long long)blockIdx.x * SF_WARPS + wp; gg < v.natoms; gg += nw) {
+    const int g = (int)gg;
+    for (int f = lane; f < SF_NF; f += 32) row[f] = 0.f;
+    __syncwarp();
+    const int I = v.inst_of[g];
+    const f4 pi = v.pos[g];
+    const int ci = v.sclass[g];
+    if (lane == 0 && ci >= 0) sf_add_shared(row, ci, 0.f);
+    int cx, cy, cz;
+    cell_of(pi.x, pi.y, pi.z, 1.0f / SF_RC, cx, cy, cz);
+    int nbuf = 0; /* warp-uniform */
+    for (int c = 0; c < 27; c++) {
+      const int ax = cx + c % 3 - 1, ay = cy + (c / 3) % 3 - 1, az = cz + c / 9 - 1;
+      const int b = v.sf_bbegin[I] + cell_hash(ax, ay, az, v.sf_bmask[I]);
+      const int key = sf_key(ax, ay, az);
+      const int s0 = v.sf_bstart[b], s1 = s0 + v.sf_bcount[b];
+      for (int q0 = s0; q0 < s1; q0 += 32) {
+        const int q = q0 + lane;
+        bool in = false;
+        float d = 0.f;
+        int cj = 0;
+        if (q < s1) {
           const int2 id = v.sf_sid[q];
           const f4 pj = v.sf_spos[q];
-          if (id.y != key || id.x == g || pj.w < 0.f) continue;
-          float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-          float d2 = dx * dx + dy * dy + dz * dz;
-          if (d2 < rc2) sf_add(row, (int)pj.w, sqrtf(d2));
+          if (id.y == key && id.x != g && pj.w >= 0.f) {
+            const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < rc2) {
+              in = true;
+              d = sqrtf(d2);
+              cj = (int)pj.w;
+            }
+          }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (in) {
+          const int pos = nbuf + __popc(m & ((1u << lane) - 1u));
+          bd[pos] = d;
+          bc[pos] = cj;
+        }
+        nbuf += __popc(m); /* at most 63 */
+        if (nbuf >= 32) {
+          __syncwarp();
+          sf_add_shared(row, bc[lane], bd[lane]);
+          __syncwarp();
+          if (lane < nbuf - 32) { /* the rest to the front (read 32 + lane, write lane) */
+            bd[lane] = bd[32 + lane];
+            bc[lane] = bc[32 + lane];
+          }
+          __syncwarp();
+          nbuf -= 32;
         }
       }
-      for (int f = 0; f < SF_NF; f++) {
-        float x = row[f];
-        if (mean) x = (x - mean[f]) * invstd[f];
-        out[(size_t)g * SF_NF + f] = __float2bfloat16(x);
-      }
     }
+    __syncwarp();
+    if (lane < nbuf) sf_add_shared(row, bc[lane], bd[lane]);
+    __syncwarp();
+    for (int f = lane; f < SF_NF; f += 32) {
+      float x = row[f];
+      if (mean) x = (x - mean[f]) * invstd[f];
+      out[(size_t)g * SF_NF + f] = __float2bfloat16(x);
+    }
+    __syncwarp(); /* the row is read before the next atom clears it */
   }
 }
 
@@ -4022,20 +4077,15 @@ extern "C" int agb_dev_surrogate_classes(agb_dev *s, const double *class_radii, 
    queued on the instance stream (which agbnp3_stream returns) */
 extern "C" int agb_dev_surrogate_features(agb_dev *s, const float *mean, const float *invstd, void *out) {
   CK(cudaSetDevice(s->device));
-  const int smem = SF_BLOCK * (SF_NF + 1) * (int)sizeof(float);
-  if (!s->sfeat_ready) {
-    CK(cudaFuncSetAttribute(k_sfeat, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    s->sfeat_ready = 1;
-  }
   View &v = s->v;
   CK(cudaMemsetAsync(v.sf_bcount, 0, sizeof(int) * v.sf_nbuckets, s->st));
   CK(cudaMemsetAsync(v.sf_bcursor, 0, sizeof(int) * v.sf_nbuckets, s->st));
   k_sf_cell_count<<<nblocks(s->natoms), BLK, 0, s->st>>>(v);
   agb_scan_excl(v.sf_bcount, v.sf_bstart, v.sf_dc, v.sf_dc + 1, v.sf_nbuckets, s->scan_scratch, s->st);
   k_sf_cell_fill<<<nblocks(s->natoms), BLK, 0, s->st>>>(v);
-  int grid = (s->natoms + SF_BLOCK - 1) / SF_BLOCK;
-  if (grid > 148 * 32) grid = 148 * 32;
-  k_sfeat<<<grid, SF_BLOCK, smem, s->st>>>(v, mean, invstd, (__nv_bfloat16 *)out);
+  int grid = (s->natoms + SF_WARPS - 1) / SF_WARPS;
+  if (grid > 148 * 16) grid = 148 * 16;
+  k_sfeat<<<grid, 32 * SF_WARPS, 0, s->st>>>(v, mean, invstd, (__nv_bfloat16 *)out);
   CK(cudaGetLastError());
   return 0;
 }

@@ -151,7 +151,8 @@ extern "C" int agbnp3_tc_gemm(const void *A, int lda, const void *B, int ldb, co
 /* ------------------------------------------------------------------------ */
 /* elementwise kernels of the MLP's training and inference                  */
 /* ------------------------------------------------------------------------ */
-__device__ __forceinline__ float silu_f(float z) { return z / (1.f + __expf(-z)); }
+/* z sigmoid(z), with the fast division (the result is rounded to bf16) */
+__device__ __forceinline__ float silu_f(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 __device__ __forceinline__ float dsilu_f(float z) {
   float s = 1.f / (1.f + __expf(-z));
   return s * (1.f + z * (1.f - s));
@@ -280,6 +281,178 @@ extern "C" int agbnp3_mlp_gather(const void *X, const float *T, const long long 
   k_mlp_gather<<<EW_GRID((long long)rows * nin), 256, 0, (cudaStream_t)stream>>>(
       (const __nv_bfloat16 *)X, T, idx, rows, nin, nout, (__nv_bfloat16 *)Xb, (__nv_bfloat16 *)Xt, ldt, Tb);
   EW_RET;
+}
+
+/* ------------------------------------------------------------------------ */
+/* fused inference: all three layers of the 160-128-128-2 SiLU network in   */
+/* one kernel.  A block of 256 threads keeps the bf16 weights in shared     */
+/* memory (canonical K-major layout) and walks 128-row tiles of the input: */
+/* X tile -> smem; layer 1 (10 MMAs of K = 16) into TMEM columns 0..127;    */
+/* bias + SiLU per row (two threads a row, tcgen05.ld), bf16 into H in      */
+/* smem; layer 2 (8 MMAs) into columns 128..255; bias + SiLU into H again;  */
+/* layer 3 (N padded to 16, 8 MMAs) into columns 0..15; bias, two outputs   */
+/* per row to global memory.  Every MMA group completes through an          */
+/* mbarrier with a bounded wait (error word, no result, TMEM freed).        */
+/* ------------------------------------------------------------------------ */
+#define MF_IN 160
+#define MF_H 128
+#define MF_OUT 2
+#define MF_N3 16 /* layer-3 MMA width (rows >= MF_OUT of W3 are zero) */
+#define MF_SMEM_W1 (MF_H * MF_IN * 2)
+#define MF_SMEM_W2 (MF_H * MF_H * 2)
+#define MF_SMEM_W3 (MF_N3 * MF_H * 2)
+#define MF_SMEM_X (128 * MF_IN * 2)
+#define MF_SMEM_H (128 * MF_H * 2)
+#define MF_SMEM (MF_SMEM_W1 + MF_SMEM_W2 + MF_SMEM_W3 + MF_SMEM_X + MF_SMEM_H + 1024)
+
+/* rows [0, rows) of a row-major bf16 matrix (leading dimension ld, `valid`
+   rows present, the rest zero) into the canonical K-major layout of an
+   rows x K tile; 16-byte chunks, one per thread per step */
+__device__ __forceinline__ void mf_stage(unsigned char *dst, const __nv_bfloat16 *__restrict__ src, int ld, int rows,
+                                         int valid, int K) {
+  const int kv = K / 8;
+  for (int e = threadIdx.x; e < rows * kv; e += blockDim.x) {
+    const int r = e / kv, k = (e % kv) * 8;
+    uint4 t = make_uint4(0, 0, 0, 0);
+    if (r < valid) t = *(const uint4 *)(src + (size_t)r * ld + k);
+    *(uint4 *)(dst + tc_off(r, k, K)) = t;
+  }
+}
+
+/* half a row of fp32 accumulators (TMEM columns c0..c0+63 of this thread's
+   lane, taddr = the lane's column 0) -> bias + SiLU -> bf16 into row r of
+   the H tile */
+__device__ __forceinline__ void mf_act_row(uint32_t taddr, const float *__restrict__ bias, unsigned char *h, int r,
+                                           int c0) {
+#pragma unroll 1
+  for (int c = c0; c < c0 + MF_H / 2; c += 16) {
+    float v[16];
+    tc_ld16(taddr + (uint32_t)c, v);
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      __align__(16) __nv_bfloat16 u[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) u[i] = __float2bfloat16(silu_f(v[8 * half + i] + bias[c + 8 * half + i]));
+      *(uint4 *)(h + tc_off(r, c + 8 * half, MF_H)) = *(const uint4 *)u;
+    }
+  }
+}
+
+/* waits for the mbarrier phase (bounded) and agrees on the outcome */
+__device__ __forceinline__ bool mf_wait(uint64_t *mbar, uint32_t &phase) {
+  bool done = tc_mbar_wait(mbar, phase, TC_WAIT_POLLS);
+  if (!done) done = tc_mbar_wait(mbar, phase, TC_WAIT_POLLS);
+  phase ^= 1u;
+  return __syncthreads_and(done);
+}
+
+#define MF_THREADS 256 /* warps w and w + 4 read TMEM lanes 32 (w % 4) .. + 31, each half of the columns */
+__global__ void __launch_bounds__(MF_THREADS, 1) k_mlp_fwd(const __nv_bfloat16 *__restrict__ X, int n,
+                                                    const __nv_bfloat16 *__restrict__ W1, const float *__restrict__ b1,
+                                                    const __nv_bfloat16 *__restrict__ W2, const float *__restrict__ b2,
+                                                    const __nv_bfloat16 *__restrict__ W3, const float *__restrict__ b3,
+                                                    float *__restrict__ Y) {
+  extern __shared__ unsigned char mf_raw[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tslot;
+  unsigned char *base = (unsigned char *)(((uintptr_t)mf_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char *sw1 = base, *sw2 = sw1 + MF_SMEM_W1, *sw3 = sw2 + MF_SMEM_W2, *sx = sw3 + MF_SMEM_W3,
+                *sh = sx + MF_SMEM_X;
+  const int tid = threadIdx.x, warp = tid >> 5, quad = warp & 3, r = 32 * quad + (tid & 31);
+  const int c0 = (warp >> 2) * (MF_H / 2); /* this thread's half of the columns */
+  mf_stage(sw1, W1, MF_IN, MF_H, MF_H, MF_IN);
+  mf_stage(sw2, W2, MF_H, MF_H, MF_H, MF_H);
+  mf_stage(sw3, W3, MF_H, MF_N3, MF_OUT, MF_H);
+  if (tid == 0) tc_mbar_init(&mbar, 1);
+  if (warp == 0) tc_alloc(&tslot, 256);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tslot, lane_off = (uint32_t)(quad * 32) << 16;
+  const uint32_t id1 = tc_idesc(128, MF_H), id3 = tc_idesc(128, MF_N3);
+  const uint32_t aw1 = tc_smem_u32(sw1), aw2 = tc_smem_u32(sw2), aw3 = tc_smem_u32(sw3), ax = tc_smem_u32(sx),
+                 ah = tc_smem_u32(sh);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int m0 = blockIdx.x * 128; m0 < n && ok; m0 += gridDim.x * 128) {
+    const int row = m0 + r; /* this thread's row: TMEM lane r */
+    mf_stage(sx, X + (size_t)m0 * MF_IN, MF_IN, 128, min(128, n - m0), MF_IN);
+    tc_fence_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      for (int kk = 0; kk < MF_IN / 16; kk++)
+        tc_mma(tmem, tc_desc(ax + kk * 256, 128, MF_IN * 16), tc_desc(aw1 + kk * 256, 128, MF_IN * 16), id1,
+               kk > 0 ? 1u : 0u);
+      tc_commit(&mbar);
+    }
+    if (!(ok = mf_wait(&mbar, phase))) break;
+    tc_fence_after();
+    mf_act_row(tmem + lane_off, b1, sh, r, c0);
+    tc_fence_before();
+    tc_fence_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      for (int kk = 0; kk < MF_H / 16; kk++)
+        tc_mma(tmem + 128, tc_desc(ah + kk * 256, 128, MF_H * 16), tc_desc(aw2 + kk * 256, 128, MF_H * 16), id1,
+               kk > 0 ? 1u : 0u);
+      tc_commit(&mbar);
+    }
+    if (!(ok = mf_wait(&mbar, phase))) break;
+    tc_fence_after();
+    mf_act_row(tmem + lane_off + 128, b2, sh, r, c0);
+    tc_fence_before();
+    tc_fence_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      for (int kk = 0; kk < MF_H / 16; kk++)
+        tc_mma(tmem, tc_desc(ah + kk * 256, 128, MF_H * 16), tc_desc(aw3 + kk * 256, 128, MF_H * 16), id3,
+               kk > 0 ? 1u : 0u);
+      tc_commit(&mbar);
+    }
+    if (!(ok = mf_wait(&mbar, phase))) break;
+    tc_fence_after();
+    if (warp < 4) {
+      float v[16];
+      tc_ld16(tmem + lane_off, v);
+      if (row < n) {
+        Y[(size_t)row * MF_OUT] = v[0] + b3[0];
+        Y[(size_t)row * MF_OUT + 1] = v[1] + b3[1];
+      }
+    }
+    tc_fence_before();
+    __syncthreads(); /* TMEM and the X tile are reused by the next tile */
+  }
+  if (!ok && tid == 0) tc_flag_error();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tc_dealloc(tmem, 256);
+}
+
+/* Y [n x 2] fp32 = the 160-128-128-2 SiLU network applied to the bf16 rows
+   of X [n x 160] (row-major), with bf16 weights W1 [128 x 160], W2
+   [128 x 128], W3 [2 x 128] (row-major, as nn.Linear stores them) and fp32
+   biases, in one launch on `stream` (not waited for; a wait that gave up
+   surfaces through agbnp3_tc_error).  X and the weights must be 16-byte
+   aligned.  Returns 0, or -1 on bad arguments or a launch error. */
+extern "C" int agbnp3_mlp_forward(const void *X, int n, const void *W1, const float *b1, const void *W2,
+                                  const float *b2, const void *W3, const float *b3, float *Y, void *stream) {
+  static int attr_set = 0;
+  if (n <= 0 || !X || !W1 || !b1 || !W2 || !b2 || !W3 || !b3 || !Y) return -1;
+  if (((uintptr_t)X | (uintptr_t)W1 | (uintptr_t)W2 | (uintptr_t)W3) & 15) return -1;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, MF_SMEM) != cudaSuccess)
+      return -1;
+    attr_set = 1;
+  }
+  int tiles = (n + 127) / 128, grid = tiles < 148 ? tiles : 148;
+  k_mlp_fwd<<<grid, MF_THREADS, MF_SMEM, (cudaStream_t)stream>>>(
+      (const __nv_bfloat16 *)X, n, (const __nv_bfloat16 *)W1, b1, (const __nv_bfloat16 *)W2, b2,
+      (const __nv_bfloat16 *)W3, b3, Y);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 /* the GEMM without waiting, for the training loop (errors surface through

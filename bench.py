@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--no-single-core", action="store_true", help="skip the 1-thread reference timing")
     p.add_argument("--cpu-best-of", type=int, default=3, help="reference evaluations per CPU baseline timing")
     p.add_argument("--no-batch", action="store_true", help="skip the 512-instance batch sub-measurement")
+    p.add_argument("--no-surrogate", action="store_true",
+                   help="skip the learned surrogate's sub-measurement (training on a reduced set, then its "
+                        "inference time, fallback and errors at 25,000 and 50,000 atoms)")
     p.add_argument("--batch-steps", type=int, default=20, help="timed steps of the batch sub-measurement")
     p.add_argument("--chosen-batch", type=int, default=4,
                    help="conformations of the globule evaluated together for the batched chosen-mode figure (<2: off)")
@@ -742,6 +745,16 @@ def main():
         batch = measure_batch(A, torch, args.ninst, args.batch_steps, 3, args.seed, rank, world, local,
                               clocks=False)
 
+    # the learned surrogate, measured (not part of the chosen mode: the
+    # figures show why)
+    sur = None
+    if rank == 0 and not args.no_surrogate:
+        try:
+            from agbnp3_b200 import surrogate as SG
+            sur = SG.bench_report()
+        except Exception as e:  # noqa: BLE001
+            sur = {"failed": str(e)}
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and os.path.exists(os.path.join(ROOT, "oracle", "_ref",
                                                                              "libagbnp3_ref.so")):
@@ -782,6 +795,7 @@ def main():
             "gpu_launches": int(st["launches"]) * args.steps,
             "roofline": roof,
             "batch512": batch,
+            "surrogate": sur,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }

@@ -98,6 +98,27 @@ def test_mlp_gradients_match_cpu_reference():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 300, 1000, 20000])
+def test_fused_forward_matches_layers(n):
+    """The one-launch network (agbnp3_mlp_forward: three tcgen05 layers, the
+    activations kept on chip) gives the layer-by-layer GEMM path's outputs:
+    the same bf16 products accumulated in fp32 and the same bf16 rounding of
+    the hidden activations, so they agree to fp32 rounding; row counts that
+    are not a multiple of the 128-row tile and several tiles per block."""
+    from agbnp3_b200 import surrogate as SG
+    net = SG.Mlp(seed=3, batch=4096)
+    for k in ("b1", "b2", "b3"):  # nonzero biases
+        net.p[k].copy_(torch.linspace(-0.5, 0.5, len(net.p[k]), device="cuda"))
+    g = torch.Generator(device="cuda").manual_seed(n)
+    X = torch.randn(n, 160, device="cuda", generator=g).to(torch.bfloat16)
+    ref = net.predict(X)
+    out = net.predict_fused(X)
+    torch.cuda.synchronize()
+    assert net.L.agbnp3_tc_error(1, None) == 0
+    assert torch.allclose(out, ref, rtol=1e-4, atol=1e-4), (out - ref).abs().max().item()
+
+
+@pytest.mark.gpu
 def test_surrogate_training_reduces_loss():
     """A short training run on FP64 labels of perturbed globule conformations
     lowers the loss and predicts held-out descreening sums better than their
@@ -127,8 +148,7 @@ def test_surrogate_gain_and_fallback():
     networks' relative error of the descreening sums is above the accuracy
     the 1e-4 energy target needs (sum_accuracy_bound), so without fallback
     the GB energy misses 1e-4, and meeting it takes most atoms back to the
-    exact sums; the
-    measured times and the gain are printed."""
+    exact sums; the measured times and the gain are printed."""
     import json
     from agbnp3_b200 import surrogate as SG
     X, T = SG.make_dataset(conformations=12, natoms=1500, bases=3, log=lambda *a: None)
@@ -137,10 +157,11 @@ def test_surrogate_gain_and_fallback():
     print(json.dumps(r))
     rows = r["rows"]
     assert rows[0]["fallback_fraction"] == 1.0 and rows[0]["egb_rel_err"] <= 1e-12
+    assert rows[0]["linearised_total_rel_err"] == 0.0
     assert rows[-1]["fallback_fraction"] == 0.0
     fr = [q["fallback_fraction"] for q in rows]
     assert all(a >= b for a, b in zip(fr, fr[1:]))
-    assert r["surrogate_ms"] > 0 and r["exact_stage_ms"] > 0
+    assert r["surrogate_ms"] > 0 and r["exact_stage_ms"] > 0 and r["features_ms"] > 0 and r["networks_ms"] > 0
     b = r["accuracy_bound"]
     assert 0.0 < b["sigma_common"] < b["sigma_random"] < r["network_rel_rms_err"]
     assert rows[-1]["egb_rel_err"] > 1e-4
