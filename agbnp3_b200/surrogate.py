@@ -12,6 +12,7 @@ one of its kernels (agbnp3_mlp_*).  torch only holds the device buffers.
     python -m agbnp3_b200.surrogate train --out model.npz [--conformations 2000 --natoms 5000]
     python -m agbnp3_b200.surrogate evaluate --model model.npz --natoms 25000
     python -m agbnp3_b200.surrogate bound [--natoms N]   (accuracy the sums need)
+    python -m agbnp3_b200.surrogate kernels --natoms N --epochs REPS   (inference kernels alone)
 
 Training data: perturbed conformations (N(0, 0.3 A) coordinate noise) of
 seeded globules, labelled by the plain FP64 path of the engine.
@@ -23,7 +24,7 @@ import time
 import numpy as np
 import torch
 
-from . import AGBNP_OK, AGBNPError, Instance, PREC_FP64, last_error, lib, make_globule
+from . import AGBNP_OK, AGBNPError, Instance, PREC_FP64, PREC_MIXED, last_error, lib, make_globule
 
 NIN, NH, NOUT = 160, 128, 2
 CLASS_RADII = (1.7, 1.55, 1.52, 1.8, 1.15)  # C, N, O, S, H (A, without the 0.5 A increment)
@@ -374,7 +375,6 @@ def gain(models, natoms, seed=1, tolerances=(0.0, 0.01, 0.03, 0.1, 0.3, float("i
     - the networks' relative RMS error of the sums against the accuracy the
       1e-4 energy target needs (sum_accuracy_bound, from the FP64 path's
       chain-rule factors)."""
-    from . import PREC_MIXED
     s = make_globule(natoms, seed)
     int2ext, _ = s.internal_order()
     radius = np.asarray(s.r)[int2ext]
@@ -434,7 +434,9 @@ def gain(models, natoms, seed=1, tolerances=(0.0, 0.01, 0.03, 0.1, 0.3, float("i
     mean, spread = P.mean(0), np.abs(P[0] - P[1]) if len(P) > 1 else np.zeros(natoms)
     # the GB energy at the surrogate's Born radii needs the allocation-free GB
     # kernel, which takes at most STATIC_MAX_ATOMS atoms; beyond that only the
-    # first-order total-energy error is reported
+    # first-order total-energy errors are reported, and the smallest fallback
+    # that meets 1e-4 is judged by their RMS over sign draws (one signed sum
+    # can cancel by chance)
     exact_gb = natoms <= STATIC_MAX_ATOMS
     e_exact = gb_energy(s, int2ext, born_radii(exact, radius)) if exact_gb else None
     rows = []
@@ -444,15 +446,18 @@ def gain(models, natoms, seed=1, tolerances=(0.0, 0.01, 0.03, 0.1, 0.3, float("i
             fall[:] = True
         S = np.where(fall, exact, mean)
         frac = float(fall.mean())
+        de = dEdS * (S - exact)  # first-order energy change of each atom's error
         row = {"tolerance": tol, "fallback_fraction": frac,
-               "linearised_total_rel_err": float(abs((dEdS * (S - exact)).sum()) / abs(e_total)),
+               "linearised_total_rel_err": float(abs(de.sum()) / abs(e_total)),
+               # the same errors with independent signs: the RMS over sign draws
+               "linearised_rms_rel_err": float(np.sqrt((de ** 2).sum()) / abs(e_total)),
                "rms_sum_err": float(np.sqrt(((S - exact) ** 2).mean()))}
         if exact_gb:
             e = gb_energy(s, int2ext, born_radii(S, radius))
             row["egb_rel_err"] = abs(e - e_exact) / abs(e_exact)
         rows.append(row)
     inst.close()
-    key = "egb_rel_err" if exact_gb else "linearised_total_rel_err"
+    key = "egb_rel_err" if exact_gb else "linearised_rms_rel_err"
     ok = [q["fallback_fraction"] for q in rows if q[key] <= 1e-4]
     return {"natoms": natoms, "surrogate_ms": t_sur, "features_ms": t_feat, "networks_ms": t_nets,
             "exact_stage_ms": t_exact,
@@ -482,7 +487,7 @@ def bench_report(sizes=(25000, 50000), conformations=60, train_atoms=5000, epoch
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["train", "evaluate", "gain", "bound"])
+    ap.add_argument("cmd", choices=["train", "evaluate", "gain", "bound", "kernels"])
     ap.add_argument("--models", nargs="*", default=[])
     ap.add_argument("--seeds", type=int, nargs="*", default=[0])
     ap.add_argument("--out", default="surrogate_model.npz")
@@ -501,6 +506,25 @@ def main():
             out = a.out.replace("{seed}", str(sd))
             np.savez(out, **model)
             print(f"saved {out}")
+    elif a.cmd == "kernels":
+        # the inference kernels alone (untrained network), for timing and
+        # profiling: features of a globule, then the fused network on them
+        s = make_globule(a.natoms, 1)
+        inst = Instance(s, precision=PREC_MIXED)
+        inst.ener()
+        set_classes(inst)
+        net = Mlp(seed=a.seed)
+        F = torch.empty(s.natoms, NIN, dtype=torch.bfloat16, device="cuda")
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        for _ in range(a.epochs):
+            e0.record()
+            features(inst, s.natoms, out=F)
+            e1.record()
+            net.predict_fused(F)
+            e2.record()
+            e2.synchronize()
+            print(f"{s.natoms} atoms: features {e0.elapsed_time(e1):.3f} ms, network {e1.elapsed_time(e2):.3f} ms")
+        inst.close()
     elif a.cmd == "bound":
         import json
         for n in (a.natoms,) if a.natoms != 5000 else (5000, 25000, 50000):
