@@ -2511,6 +2511,7 @@ struct agb_dev {
   cudaEvent_t ev[AGB_NSTAGE + 1];
   cudaStream_t st2;                /* side stream of the water-site stage */
   cudaEvent_t fork_ev, join_ev;    /* orders st2 against st */
+  cudaEvent_t tfork_ev, tjoin_ev;  /* the tree-derivative orders split over st and st2 */
   cudaEvent_t xev; /* orders the instance stream against a caller's stream */
   double stage_ms[AGB_NSTAGE];
   long long nlaunch;
@@ -2782,6 +2783,8 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
   CK(cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&s->tfork_ev, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&s->tjoin_ev, cudaEventDisableTiming));
   View &v = s->v;
   memset(&v, 0, sizeof(v));
   int N = d->natoms, NI = d->ninst, NW = d->nws;
@@ -3058,6 +3061,8 @@ extern "C" void agb_dev_destroy(agb_dev *s) {
     if (s->ev[k]) cudaEventDestroy(s->ev[k]);
   if (s->fork_ev) cudaEventDestroy(s->fork_ev);
   if (s->join_ev) cudaEventDestroy(s->join_ev);
+  if (s->tfork_ev) cudaEventDestroy(s->tfork_ev);
+  if (s->tjoin_ev) cudaEventDestroy(s->tjoin_ev);
   if (s->st2) cudaStreamDestroy(s->st2);
   if (s->xev) cudaEventDestroy(s->xev);
   cudaStreamDestroy(s->st);
@@ -3437,14 +3442,29 @@ static void launch_all(agb_dev *s, int seg = -1) {
     nl += 4 + AGB_SCAN_LAUNCHES;
   }
   stage_mark(s, 8);
-  for (int m = 2; m <= AGB_MAX_ORDER; m++) {
-    switch (m) {
-      case 2: AGB_LAUNCH((k_tree_ders<R, 2>), nblocks(v.cap[m]), BLK, st, v); break;
-      case 3: AGB_LAUNCH((k_tree_ders<R, 3>), nblocks(v.cap[m]), BLK, st, v); break;
-      case 4: AGB_LAUNCH((k_tree_ders<R, 4>), nblocks(v.cap[m]), BLK, st, v); break;
-      default: AGB_LAUNCH((k_tree_ders<R, 5>), nblocks(v.cap[m]), BLK, st, v); break;
+  if (!s->timing && seg < 0) {
+    /* the orders are independent (each reads its own records and adds to
+       the gradients with atomics): orders 3 and 5 on the side stream beside
+       2 and 4, which splits the records about evenly and fills the tails */
+    cudaEventRecord(s->tfork_ev, st);
+    cudaStreamWaitEvent(s->st2, s->tfork_ev, 0);
+    AGB_LAUNCH((k_tree_ders<R, 3>), nblocks(v.cap[3]), BLK, s->st2, v);
+    AGB_LAUNCH((k_tree_ders<R, 5>), nblocks(v.cap[5]), BLK, s->st2, v);
+    cudaEventRecord(s->tjoin_ev, s->st2);
+    AGB_LAUNCH((k_tree_ders<R, 2>), nblocks(v.cap[2]), BLK, st, v);
+    AGB_LAUNCH((k_tree_ders<R, 4>), nblocks(v.cap[4]), BLK, st, v);
+    cudaStreamWaitEvent(st, s->tjoin_ev, 0);
+    nl += 4;
+  } else {
+    for (int m = 2; m <= AGB_MAX_ORDER; m++) {
+      switch (m) {
+        case 2: AGB_LAUNCH((k_tree_ders<R, 2>), nblocks(v.cap[m]), BLK, st, v); break;
+        case 3: AGB_LAUNCH((k_tree_ders<R, 3>), nblocks(v.cap[m]), BLK, st, v); break;
+        case 4: AGB_LAUNCH((k_tree_ders<R, 4>), nblocks(v.cap[m]), BLK, st, v); break;
+        default: AGB_LAUNCH((k_tree_ders<R, 5>), nblocks(v.cap[m]), BLK, st, v); break;
+      }
+      nl += 1;
     }
-    nl += 1;
   }
   stage_mark(s, 9);
   AGB_LAUNCH(k_final, nblocks(N), BLK, st, v);
