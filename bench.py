@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--no-single-core", action="store_true", help="skip the 1-thread reference timing")
     p.add_argument("--cpu-best-of", type=int, default=3, help="reference evaluations per CPU baseline timing")
     p.add_argument("--no-batch", action="store_true", help="skip the 512-instance batch sub-measurement")
+    p.add_argument("--no-large", action="store_true",
+                   help="skip the 100,000-atom sub-measurement (chosen mode, plain FP64, per-term error)")
     p.add_argument("--no-surrogate", action="store_true",
                    help="skip the learned surrogate's sub-measurement (training on a reduced set, then its "
                         "inference time, fallback and errors at 25,000 and 50,000 atoms)")
@@ -497,6 +499,48 @@ def measure_conformations(A, torch, s, k, steps, warmup, local, world, full, tot
     return out
 
 
+def measure_large(A, torch, natoms, seed, steps, steps64, local, world):
+    """One large globule (configs' mixed-precision case): the chosen mode and
+    the plain FP64 path, each autotuned, device-timed over `steps` / `steps64`
+    evaluations (L2 flushed between them), and the chosen mode's per-term
+    error against the FP64 path."""
+    from agbnp3_b200.shard import max_over_ranks, throughput
+    s = A.make_globule(natoms, seed)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    res = {}
+    for prec, k, n in ((A.PREC_MIXED, "mixed", steps), (A.PREC_FP64, "fp64", steps64)):
+        inst = A.Instance(s, precision=prec, compat=True)
+        inst.ener()
+        inst.set_coords(s.coords())
+        tune = inst.autotune()
+        stream = torch.cuda.ExternalStream(inst.stream, device=torch.device("cuda", local))
+        inst.ener_resident()
+        times = []
+        for _ in range(n):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            inst.ener_resident()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        t = max_over_ranks(sum(times), world, f"cuda:{local}")
+        res[k] = {"value": throughput(n, t / 1e3, world), "ms_per_step": t / n, "steps": n, "autotune": tune,
+                  "out": inst.results()}
+        inst.close()
+    M, F = res["mixed"].pop("out"), res["fp64"].pop("out")
+    tot = lambda R: sum(R[q] for q in ("egb", "evdw", "ecav", "ehb"))  # noqa: E731
+    frc = lambda R: R["dgbdr"] + R["dvwdr"] + R["decav"] + R["dehb"]  # noqa: E731
+    return {"workload": workload_name(natoms, s.nheavy, seed), "unit": UNIT, "mixed": res["mixed"],
+            "fp64_plain": res["fp64"], "speedup_of_chosen": res["mixed"]["value"] / res["fp64"]["value"],
+            "accuracy_vs_fp64": {"energy_rel_err": abs(tot(M) - tot(F)) / abs(tot(F)),
+                                 "force_rms_rel_err": float(np.sqrt(((frc(M) - frc(F)) ** 2).sum() / (frc(F) ** 2).sum())),
+                                 "per_term_rel_err": {q: abs(M[q] - F[q]) / max(abs(F[q]), 1e-12)
+                                                      for q in ("egb", "evdw", "ecav", "ehb", "mol_volume")}}}
+
+
 def batch_main(args, A, torch, rank, world, local):
     """512 independent instances (log-uniform 300-5,000 atoms, 0.2 A noise)
     evaluated together: one step = one batched evaluation of all instances;
@@ -745,6 +789,11 @@ def main():
         batch = measure_batch(A, torch, args.ninst, args.batch_steps, 3, args.seed, rank, world, local,
                               clocks=False)
 
+    # the 100,000-atom globule (mixed-precision configuration), same run
+    large = None
+    if not args.no_large and natoms != 100000:
+        large = measure_large(A, torch, 100000, args.seed, 10, 3, local, world)
+
     # the learned surrogate, measured (not part of the chosen mode: the
     # figures show why)
     sur = None
@@ -795,6 +844,7 @@ def main():
             "gpu_launches": int(st["launches"]) * args.steps,
             "roofline": roof,
             "batch512": batch,
+            "globule100k": large,
             "surrogate": sur,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
