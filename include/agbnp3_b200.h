@@ -236,6 +236,17 @@ int agbnp3_mlp_adam(float *p, const float *g, float *m, float *v, long long n, f
 int agbnp3_mlp_pack(const float *W, int N, int K, void *Wb, void *Wt, int ldt, void *stream);
 int agbnp3_mlp_gather(const void *X, const float *T, const long long *idx, int rows, int nin, int nout, void *Xb,
                       void *Xt, int ldt, float *Tb, void *stream);
+/* Inference of the whole 160-128-128-2 SiLU network in one launch: Y [n][2]
+   fp32 for bf16 rows X [n][160], bf16 weights W1 [128][160], W2 [128][128],
+   W3 [2][128] (row-major) and fp32 biases, all device arrays, X and the
+   weights 16-byte aligned.  The weights stay in shared memory, each layer
+   is a group of tcgen05 MMAs into tensor memory and its bias and SiLU go
+   straight from tensor memory into the next layer's operand.  Queued on
+   `stream` (not waited for; an MMA wait that gave up surfaces through
+   agbnp3_tc_error).  Returns 0, or -1 on bad arguments or a launch error.
+   No counterpart in the reference. */
+int agbnp3_mlp_forward(const void *X, int n, const void *W1, const float *b1, const void *W2, const float *b2,
+                       const void *W3, const float *b3, float *Y, void *stream);
 
 /* Arithmetic peaks of GPU `device` measured by the library's own
    throughput kernels (about 0.1 s): out[0] FP32 flop/s counting an FMA as
