@@ -88,6 +88,34 @@ def test_near_list_bit_exact(engine, name, prec):
         inst.close()
 
 
+def test_near_list_warp_search(engine, monkeypatch, large25k):
+    """The near-list search used for large systems (a warp per 32 grid slots
+    and neighbour direction, AGBNP3_NL_CELLS=1 forces it here) gives the
+    reference's list too: the golden cases and the 25,000-atom globule
+    (counts and the digest of the lists in the reference's order)."""
+    from conftest import array_digest
+    monkeypatch.setenv("AGBNP3_NL_CELLS", "1")
+    for name in GOLDEN_CASES:
+        s, d = load_golden(name)
+        inst = A.Instance(s, precision=A.PREC_MIXED)
+        try:
+            inst.ener()
+            cnt, lst = inst.near_list()
+            assert np.array_equal(cnt[: s.nheavy], d["nl_count"]), name
+            assert np.array_equal(lst, d["nl_list"]), name
+        finally:
+            inst.close()
+    s, d, _ = large25k
+    inst = A.Instance(s, precision=A.PREC_FP64)
+    try:
+        inst.ener()
+        cnt, lst = inst.near_list()
+        assert np.array_equal(cnt[: s.nheavy], d["nl_count"])
+        assert len(lst) == int(d["nl_total"]) and array_digest(lst, "i4") == str(d["nl_digest"])
+    finally:
+        inst.close()
+
+
 def canonical(parents):
     return {tuple(sorted(p)) for p in parents.tolist()}
 
