@@ -164,7 +164,10 @@ enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m
 
 /* record fields of a kept overlap, stored contiguously per record (12
    slots, three 4-wide vectors) */
-enum { F_A = 0, F_P, F_CX, F_CY, F_CZ, F_GVOL, F_GVOLP, F_FP, F_FPP, F_NUM = 12 };
+/* a kept overlap's record: the product Gaussian (a, p, centre), its raw
+   volume and the switch derivatives; the switched volume is used only when
+   the overlap is made and is not stored */
+enum { F_A = 0, F_P, F_CX, F_CY, F_CZ, F_GVOL, F_FP, F_FPP, F_NUM = 8 };
 
 /* packed per-atom operands, in the working precision: position, 1/R,
    1/(h R), Gaussian exponent KFC/R^2, sp, charge, B, 1/B, q2ab, abrw.
@@ -740,18 +743,16 @@ template <typename R>
 __device__ __forceinline__ void rec_put(const View &v, int m, int q, const Ov<R> &o) {
   R *b = (R *)v.rec[m] + (size_t)q * F_NUM;
   Vec4<R>::st(b, o.a, o.p, o.cx, o.cy);
-  Vec4<R>::st(b + 4, o.cz, o.gvol, o.gvolp, o.fp);
-  Vec4<R>::st(b + 8, o.fpp, R(0), R(0), R(0));
+  Vec4<R>::st(b + 4, o.cz, o.gvol, o.fp, o.fpp);
 }
 
 template <typename R>
 __device__ __forceinline__ Ov<R> rec_load(const View &v, int m, int q) {
   const R *b = (const R *)v.rec[m] + (size_t)q * F_NUM;
   Ov<R> o;
-  R pad;
   Vec4<R>::ld(b, o.a, o.p, o.cx, o.cy);
-  Vec4<R>::ld(b + 4, o.cz, o.gvol, o.gvolp, o.fp);
-  Vec4<R>::ld(b + 8, o.fpp, pad, pad, pad);
+  Vec4<R>::ld(b + 4, o.cz, o.gvol, o.fp, o.fpp);
+  o.gvolp = R(0); /* not stored */
   return o;
 }
 

@@ -235,7 +235,7 @@ def tree_roofline(natoms, nheavy, counts, stage_ms, hbm_gbs, rbytes, traffic):
                 (8 B) out;
       volumes:  near-list entries (4 B) and per-atom Gaussian operands
                 (x, y, z, exponent, 1/R: 5 R) in; per kept overlap one
-                12-slot record (12 R) and its parents (4 B each) out, plus
+                8-slot record (8 R) and its parents (4 B each) out, plus
                 the per-atom volume and area (16 B);
       ws:       positions of all atoms (3 R) and heavy-atom scaling
                 factors (8 B) in; per water site its position (3 R), its
@@ -249,7 +249,7 @@ def tree_roofline(natoms, nheavy, counts, stage_ms, hbm_gbs, rbytes, traffic):
     P = counts["near_pairs"]
     K = counts["kept"]
     nws = counts["water_sites"]
-    rec = sum(k * (12 * R + 4 * m) for m, k in zip(range(2, 6), K))
+    rec = sum(k * (8 * R + 4 * m) for m, k in zip(range(2, 6), K))
     alg = {"nblist": 16 * nheavy + 8 * P + 8 * nheavy,
            "volumes": 4 * P + 5 * R * natoms + rec + 16 * nheavy,
            "ws": 3 * R * natoms + 8 * nheavy + nws * (39 * R + 16),

@@ -110,7 +110,7 @@ def test_tree_roofline(bench):
                       "k_tree_ders<float, 2>": {"dram_bytes_per_eval": 3e6}}}
     r = bench.tree_roofline(25000, 12500, counts, stage, 6500.0, 4, tr)
     assert r["nblist"]["alg_bytes"] == 16 * 12500 + 8 * 300000 + 8 * 12500
-    rec = sum(k * (48 + 4 * m) for m, k in zip(range(2, 6), counts["kept"]))
+    rec = sum(k * (32 + 4 * m) for m, k in zip(range(2, 6), counts["kept"]))
     assert r["treeders"]["alg_bytes"] == rec + 32 * 12500 + 96 * 25000
     for k, e in r.items():
         assert e["achieved_gbs"] == pytest.approx(e["alg_bytes"] / (stage[k] * 1e-3) / 1e9)
