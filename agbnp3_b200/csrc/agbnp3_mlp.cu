@@ -440,13 +440,17 @@ __global__ void __launch_bounds__(MF_THREADS, 1) k_mlp_fwd(const __nv_bfloat16 *
    aligned.  Returns 0, or -1 on bad arguments or a launch error. */
 extern "C" int agbnp3_mlp_forward(const void *X, int n, const void *W1, const float *b1, const void *W2,
                                   const float *b2, const void *W3, const float *b3, float *Y, void *stream) {
-  static int attr_set = 0;
+  /* the shared-memory limit is raised once per device (an attribute of the
+     function on the current device); setting it twice is harmless */
+  static int attr_set[64];
   if (n <= 0 || !X || !W1 || !b1 || !W2 || !b2 || !W3 || !b3 || !Y) return -1;
   if (((uintptr_t)X | (uintptr_t)W1 | (uintptr_t)W2 | (uintptr_t)W3) & 15) return -1;
-  if (!attr_set) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+  if (!attr_set[dev]) {
     if (cudaFuncSetAttribute(k_mlp_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, MF_SMEM) != cudaSuccess)
       return -1;
-    attr_set = 1;
+    attr_set[dev] = 1;
   }
   int tiles = (n + 127) / 128, grid = tiles < 148 ? tiles : 148;
   k_mlp_fwd<<<grid, MF_THREADS, MF_SMEM, (cudaStream_t)stream>>>(
