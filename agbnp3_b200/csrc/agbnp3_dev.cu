@@ -1122,7 +1122,10 @@ __global__ void k_pack_sp(View v) {
 }
 
 /* partner range of a work item: chunk w.w of nch of [p0, p1) */
-__device__ __forceinline__ void chunk_range(int p0, int p1, int c, int nch, int &c0, int &c1) {
+/* partner range [c0, c1) of an item's chunk: the item's code holds its
+   chunk index c and its instance's chunk count n as c + 64 n */
+__device__ __forceinline__ void chunk_range(int p0, int p1, int code, int &c0, int &c1) {
+  const int c = code & 63, nch = code >> 6;
   long long len = p1 - p0;
   c0 = p0 + (int)(len * c / nch);
   c1 = p0 + (int)(len * (c + 1) / nch);
@@ -1292,7 +1295,7 @@ __global__ void __launch_bounds__(ITILE / 2, DescBlocks<R>::v) k_descreen_t(View
       __syncwarp();
     }
     int p0 = v.inst_begin[w.x], c0, c1;
-    chunk_range(p0, p0 + v.inst_nheavy[w.x], w.w, nch, c0, c1);
+    chunk_range(p0, p0 + v.inst_nheavy[w.x], w.w, c0, c1);
     for (int j0 = c0; j0 < c1; j0 += ITILE) {
       int n = min(ITILE, c1 - j0);
       const int T0 = j0 >> 5, ntl = ((j0 + n - 1) >> 5) - T0 + 1; /* ntl <= 5 */
@@ -1390,7 +1393,7 @@ __global__ void __launch_bounds__(ITILE) k_agb_t(View v, const int4 *__restrict_
     int g = w.y + threadIdx.x;
     bool act = g < w.z;
     int c0, c1;
-    chunk_range(v.inst_begin[w.x], v.inst_begin[w.x + 1], w.w, nch, c0, c1);
+    chunk_range(v.inst_begin[w.x], v.inst_begin[w.x + 1], w.w, c0, c1);
     double df = v.inst_df[w.x];
     R xg = act ? X[g] : R(0), yg = act ? Y[g] : R(0), zg = act ? Z[g] : R(0);
     R bg = act ? Bv[g] : R(1), cg = act ? GbExp<R>::scale() * BI[g] : R(0);
@@ -1485,7 +1488,7 @@ __global__ void __launch_bounds__(ITILE) k_gbders_t(View v, const int4 *__restri
     int a0 = v.inst_begin[w.x], hh = a0 + v.inst_nheavy[w.x], a1 = v.inst_begin[w.x + 1];
     /* a tile of hydrogens only needs heavy partners */
     int c0, c1;
-    chunk_range(a0, w.y >= hh ? hh : a1, w.w, nch, c0, c1);
+    chunk_range(a0, w.y >= hh ? hh : a1, w.w, c0, c1);
     bool heavy = g < hh;
     R xg = act ? X[g] : R(0), yg = act ? Y[g] : R(0), zg = act ? Z[g] : R(0);
     R rhg = act ? RH[g] : R(0), spg = act ? SP[g] : R(0);
@@ -2754,19 +2757,33 @@ static int build_items(agb_dev *s, int nch, int jb) {
   if (jb < 1) jb = 1;
   s->nch = nch;
   s->jb = jb;
-  int nit = ntiles * nch;
-  int4 *it = (int4 *)malloc(sizeof(int4) * nit);
+  /* chunks of about the same length in every instance: the largest
+     instance's heavy atoms in nch chunks, a smaller one in fewer (a small
+     instance split as finely would spend its items on their set-up) */
+  int maxh = 1;
+  for (int I = 0; I < NI; I++)
+    if (inh[I] > maxh) maxh = inh[I];
+  const int clen = (maxh + nch - 1) / nch;
+  int *nchi = (int *)malloc(sizeof(int) * (NI > 0 ? NI : 1));
+  int nit = 0;
+  for (int I = 0; I < NI; I++) {
+    int c = (inh[I] + clen - 1) / clen;
+    nchi[I] = c < 1 ? 1 : (c > nch ? nch : c);
+    nit += ((ib[I + 1] - ib[I] + ITILE - 1) / ITILE) * nchi[I];
+  }
+  int4 *it = (int4 *)malloc(sizeof(int4) * (nit > 0 ? nit : 1));
   int q = 0;
   for (int I = 0; I < NI; I++)
     for (int a = ib[I]; a < ib[I + 1]; a += ITILE)
-      for (int c = 0; c < nch; c++) {
+      for (int c = 0; c < nchi[I]; c++) {
         int e = a + ITILE < ib[I + 1] ? a + ITILE : ib[I + 1];
         it[q].x = I;
         it[q].y = a;
         it[q].z = e;
-        it[q].w = c;
+        it[q].w = c + 64 * nchi[I]; /* chunk c of nchi[I] (chunk_range) */
         q++;
       }
+  free(nchi);
   /* symmetric items: i blocks of SymNI<R> 32-atom tiles for the precision,
      runs of up to jb 32-atom j tiles from the block's first tile to the
      end of the instance */
