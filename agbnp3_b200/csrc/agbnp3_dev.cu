@@ -2203,21 +2203,29 @@ __device__ __forceinline__ int ws_cell_scan(const View &v, int w, int c, int *ou
   return m;
 }
 
+/* one thread per (site, neighbour cell), taken direction-major: the lanes
+   of a warp are consecutive sites (of nearby parents) looking in the same
+   direction, so they mostly walk the same or neighbouring buckets; counts
+   and offsets stay in (site, cell) order */
 template <typename R>
 __global__ void k_ws_count27(View v) {
-  AGB_GRID_STRIDE(q, 27LL * v.nws) { v.ws_c27[q] = ws_cell_scan<R>(v, (int)(q / 27), (int)(q % 27), NULL, 0); }
+  AGB_GRID_STRIDE(q, 27LL * v.nws) {
+    const int c = (int)(q / v.nws), w = (int)(q % v.nws);
+    v.ws_c27[27 * w + c] = ws_cell_scan<R>(v, w, c, NULL, 0);
+  }
 }
 
 template <typename R>
 __global__ void k_ws_emit27(View v) {
   AGB_GRID_STRIDE(q, 27LL * v.nws) {
-    int n = v.ws_c27[q], o = v.ws_o27[q];
+    const int c = (int)(q / v.nws), w = (int)(q % v.nws);
+    int n = v.ws_c27[27 * w + c], o = v.ws_o27[27 * w + c];
     if (n == 0) continue;
     if (o + n > v.cap_wsc) {
       set_err(v, AGB_ERR_WS_CAP);
       continue;
     }
-    ws_cell_scan<R>(v, (int)(q / 27), (int)(q % 27), v.ws_cand + o, n);
+    ws_cell_scan<R>(v, w, c, v.ws_cand + o, n);
   }
 }
 
