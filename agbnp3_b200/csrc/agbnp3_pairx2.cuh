@@ -339,14 +339,14 @@ __device__ __forceinline__ void gbd_tile_x2(const GxI &I, GxP &P, GxJ &J, const 
       P.vx[p] = fma2(ut, dx[p], P.vx[p]);
       P.vy[p] = fma2(ut, dy[p], P.vy[p]);
       P.vz[p] = fma2(ut, dz[p], P.vz[p]);
-      const float2 hx = mul2(ht, dx[p]), hy = mul2(ht, dy[p]), hz = mul2(ht, dz[p]);
-      const float2 ux = mul2(ut, dx[p]), uy = mul2(ut, dy[p]), uz = mul2(ut, dz[p]);
-      J.fx -= hx.x + hx.y;
-      J.fy -= hy.x + hy.y;
-      J.fz -= hz.x + hz.y;
-      J.vx -= ux.x + ux.y;
-      J.vy -= uy.x + uy.y;
-      J.vz -= uz.x + uz.y;
+      /* the j atom takes the opposite of both halves' terms: two fused
+         multiply-adds per component */
+      J.fx = fmaf(-ht.x, dx[p].x, fmaf(-ht.y, dx[p].y, J.fx));
+      J.fy = fmaf(-ht.x, dy[p].x, fmaf(-ht.y, dy[p].y, J.fy));
+      J.fz = fmaf(-ht.x, dz[p].x, fmaf(-ht.y, dz[p].y, J.fz));
+      J.vx = fmaf(-ut.x, dx[p].x, fmaf(-ut.y, dx[p].y, J.vx));
+      J.vy = fmaf(-ut.x, dy[p].x, fmaf(-ut.y, dy[p].y, J.vy));
+      J.vz = fmaf(-ut.x, dz[p].x, fmaf(-ut.y, dz[p].y, J.vz));
     }
     if (TWO) {
       J.U = rot1(J.U);
