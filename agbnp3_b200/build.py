@@ -1,6 +1,8 @@
 """Builds the in-tree shared libraries of the package:
 
 - libagbnp3_b200.so : the engine (C host layer + sm_100a CUDA kernels)
+- libagbnp3_b200_sp.so : the same engine with the reference's float interface
+  (its entry points built with SINGLE_PREC_INTERFACE: float_i = float)
 - libagbnp3_globule.so : the seeded synthetic-globule generator
 
 Usage: python -m agbnp3_b200.build  (or __graft_entry__.build()).
@@ -15,6 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 INC = os.path.join(ROOT, "include")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libagbnp3_b200.so")
+LIB_SP = os.path.join(HERE, "libagbnp3_b200_sp.so")
 GLOBULE = os.path.join(HERE, "libagbnp3_globule.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -60,6 +63,15 @@ def build(force=False, verbose=False):
                              "-I", "/usr/local/cuda/include", "-c", src, "-o", obj]))
     if force or _stale(LIB, objs):
         log.append(_run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs, "-ldl"]))
+    # the float-interface library: the host layer again with float_i = float
+    src = os.path.join(CSRC, "agbnp3_host.c")
+    obj_sp = os.path.join(BUILD, "agbnp3_host_sp.c.o")
+    if force or _stale(obj_sp, [src] + hdrs):
+        log.append(_run(["gcc", "-O2", "-fPIC", "-std=c11", "-Wall", "-DSINGLE_PREC_INTERFACE", "-I", CSRC, "-I", INC,
+                         "-I", "/usr/local/cuda/include", "-c", src, "-o", obj_sp]))
+    objs_sp = [obj_sp if o.endswith("agbnp3_host.c.o") else o for o in objs]
+    if force or _stale(LIB_SP, objs_sp):
+        log.append(_run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB_SP, *objs_sp, "-ldl"]))
     gsrc = os.path.join(CSRC, "globule.c")
     if force or _stale(GLOBULE, [gsrc]):
         log.append(_run(["gcc", "-O2", "-shared", "-fPIC", "-o", GLOBULE, gsrc, "-lm"]))

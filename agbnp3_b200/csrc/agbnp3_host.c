@@ -59,6 +59,7 @@ typedef struct {
   float cell;
   int precision, compat, device, verbose;
   agb_dev *dev;
+  double *stage; /* float interface: double copies of coordinates and outputs (15 natoms) */
 } inst_t;
 
 typedef struct {
@@ -119,7 +120,7 @@ static void inst_free(inst_t *I) {
   if (I->dev) agb_dev_destroy(I->dev);
   void *ps[] = {I->int2ext, I->ext2int, I->r,       I->charge,    I->igamma,  I->sgamma,   I->ialpha,
                 I->salpha,  I->hbcorr,  I->hbtype,  I->conn_off,  I->conn_list, I->rtype,  I->tab,
-                I->ws_kind, I->ws_parent, I->ws_nparent, I->ws_prev, I->ws_khb};
+                I->ws_kind, I->ws_parent, I->ws_nparent, I->ws_prev, I->ws_khb, I->stage};
   for (size_t k = 0; k < sizeof(ps) / sizeof(ps[0]); k++) free(ps[k]);
   free(I);
 }
@@ -550,11 +551,11 @@ int agbnp3_new(int *tag, int natoms, float_i *x, float_i *y, float_i *z, float_i
   free(ish);
 
   double **dst[] = {&I->r, &I->charge, &I->igamma, &I->sgamma, &I->ialpha, &I->salpha, &I->hbcorr};
-  double *src[] = {r, charge, igamma, sgamma, ialpha, salpha, hbcorr};
+  const float_i *src[] = {r, charge, igamma, sgamma, ialpha, salpha, hbcorr};
   for (int k = 0; k < 7; k++) {
     *dst[k] = (double *)malloc(sizeof(double) * N);
     if (!*dst[k]) goto oom;
-    for (int i = 0; i < N; i++) (*dst[k])[i] = src[k][I->int2ext[i]];
+    for (int i = 0; i < N; i++) (*dst[k])[i] = (double)src[k][I->int2ext[i]];
   }
   /* the radius increment of agbnp3.c:210 */
   for (int i = 0; i < N; i++) I->r[i] += H_RINC;
@@ -696,17 +697,55 @@ int agbnp3_ener(int tag, int init, float_i *x, float_i *y, float_i *z, float_i *
     errprint("agbnp3_ener(): NULL coordinates.");
     return AGBNP_ERR;
   }
+  double e[7];
+#ifdef SINGLE_PREC_INTERFACE
+  /* float arrays in and out through double copies */
+  const int N = I->natoms;
+  if (!I->stage && !(I->stage = (double *)malloc(sizeof(double) * 15 * (size_t)N))) {
+    errprint("agbnp3_ener(): out of memory.");
+    return AGBNP_ERR;
+  }
+  double *sx = I->stage, *sy = sx + N, *sz = sy + N;
+  for (int i = 0; i < N; i++) {
+    sx[i] = x[i];
+    sy[i] = y[i];
+    sz[i] = z[i];
+  }
+  if (agb_dev_upload_coords(I->dev, sx, sy, sz) != 0) {
+    errprint("agbnp3_ener(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  if (eval_dev(I->dev, "agbnp3_ener()") != AGBNP_OK) return AGBNP_ERR;
+  double *osp = I->stage, *obr = osp + N, *osa = obr + N, *ogb = osa + N, *ogv = ogb + 3 * (size_t)N,
+         *ogc = ogv + 3 * (size_t)N, *ogh = ogc + 3 * (size_t)N;
+  if (agb_dev_download(I->dev, e, sp ? osp : NULL, br ? obr : NULL, surf_area ? osa : NULL, dgbdr ? ogb : NULL,
+                       dvwdr ? ogv : NULL, decav ? ogc : NULL, dehb ? ogh : NULL) != 0) {
+    errprint("agbnp3_ener(): %s", agb_dev_last_error());
+    return AGBNP_ERR;
+  }
+  float_i *o1[] = {sp, br, surf_area};
+  const double *d1[] = {osp, obr, osa};
+  for (int k = 0; k < 3; k++)
+    if (o1[k])
+      for (int i = 0; i < N; i++) o1[k][i] = (float_i)d1[k][i];
+  float_i(*o3[])[3] = {dgbdr, dvwdr, decav, dehb};
+  const double *d3[] = {ogb, ogv, ogc, ogh};
+  for (int k = 0; k < 4; k++)
+    if (o3[k])
+      for (int i = 0; i < N; i++)
+        for (int c = 0; c < 3; c++) o3[k][i][c] = (float_i)d3[k][3 * i + c];
+#else
   if (agb_dev_upload_coords(I->dev, x, y, z) != 0) {
     errprint("agbnp3_ener(): %s", agb_dev_last_error());
     return AGBNP_ERR;
   }
   if (eval_dev(I->dev, "agbnp3_ener()") != AGBNP_OK) return AGBNP_ERR;
-  double e[7];
   if (agb_dev_download(I->dev, e, sp, br, surf_area, (double *)dgbdr, (double *)dvwdr, (double *)decav,
                        (double *)dehb) != 0) {
     errprint("agbnp3_ener(): %s", agb_dev_last_error());
     return AGBNP_ERR;
   }
+#endif
   if (egb) *egb = e[0];
   if (evdw) *evdw = e[1];
   if (ecorr_vdw) *ecorr_vdw = e[2];

@@ -23,11 +23,14 @@ extern "C" {
 #define TRUE 1
 #endif
 
-/* interface floating-point type (agbnp3.h:44-50) */
+/* interface floating-point type (agbnp3.h:44-50): double, or float for a
+   caller built with SINGLE_PREC_INTERFACE, which links libagbnp3_b200_sp.so
+   (the same engine built with that define: its entry points take float
+   arrays and convert them; the evaluation is the same) */
 #ifndef FLOAT_I_H
 #define FLOAT_I_H
 #ifdef SINGLE_PREC_INTERFACE
-#error "libagbnp3_b200 is built with the default double interface (float_i = double)"
+typedef float float_i;
 #else
 typedef double float_i;
 #endif
