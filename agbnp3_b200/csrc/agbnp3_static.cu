@@ -2,9 +2,8 @@
  * GB energy at given Born radii without any device allocation.
  *
  * Some callers cannot call cudaMalloc: host MD codes that own all device
- * memory through their own pool and forbid other allocations, code running
- * inside a stream capture that a CUDA graph will replay, or plugins whose
- * memory budget is fixed up front.  This entry point serves them: it runs
+ * memory through their own pool and forbid other allocations, or plugins
+ * whose memory budget is fixed up front.  This entry point serves them: it runs
  * the GB pair stage of the engine (agbnp3_cpu_simd_kernels.c:66-151,
  * 329-460) on device arrays the caller passes, and keeps its scratch (the
  * packed float operands and the per-atom energy terms) in one file-scope

@@ -170,8 +170,7 @@ int agbnp3_batch_stage_times(int btag, double *ms, int n);
    arrays are device pointers and `stream` is a cudaStream_t (NULL: the
    default stream).  It allocates no device memory: for callers that cannot
    call cudaMalloc (an MD code that owns all device memory through its own
-   pool, work recorded into a CUDA graph, a plugin with a fixed memory
-   budget).  Its scratch is a static device array sized for at most 32768
+   pool, a plugin with a fixed memory budget).  Its scratch is a static device array sized for at most 32768
    atoms, held by every GPU that loads the library until exit; larger
    systems are rejected with AGBNP_ERR.  The first call on each device
    looks the array up with that device current and should come before any

@@ -1,8 +1,8 @@
 """The allocation-free GB energy entry point (agbnp3_gb_energy_static).
 
 It is meant for callers that cannot call cudaMalloc (a host MD code that
-owns all device memory, work recorded into a CUDA graph, a plugin with a
-fixed memory budget).  Called through the C-ABI on device arrays, twice in
+owns all device memory through its own pool, a plugin with a fixed memory
+budget).  Called through the C-ABI on device arrays, twice in
 a row, it must agree with the engine's own GB pair stage of agbnp3_ener:
 the GB energy (which depends only on coordinates, charges and Born radii)
 and the A_i terms, within the mixed-precision tolerances of the parity
