@@ -498,11 +498,16 @@ __global__ void k_nl_cells(View v) {
 
 /* each atom's list in (float d^2, index) order (agbnp3.c:3766-3792,
    4062-4066), one warp per atom: lane c < 27 copies its cell's sub-slab to
-   the atom's range of the list (placed by the scan of the per-cell
-   counts), then every entry is written at its rank */
+   the warp's buffer in shared memory (to the atom's range of the list in
+   global memory when it holds more than NLR_BUF entries), at the place the
+   warp's scan of the per-cell counts gives, then every entry is written at
+   its rank; the list starts where the scan of all counts places it */
+#define NLR_BUF 64 /* near-list entries of an atom ranked in shared memory */
 __global__ void k_nl_rank27(View v) {
   if (v.dc[DC_ERR] & AGB_ERR_NL_CAP) return;
-  const int lane = threadIdx.x & 31;
+  __shared__ int sj[BLK / 32][NLR_BUF];
+  __shared__ float sd[BLK / 32][NLR_BUF];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long g = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < v.natoms; g += nw) {
     const int cnt = lane < 27 ? v.nl_c27[27 * g + lane] : 0;
@@ -523,6 +528,26 @@ __global__ void k_nl_rank27(View v) {
       continue;
     }
     const size_t sb = ((size_t)g * 27 + lane) * v.slab_w;
+    if (m <= NLR_BUF) { /* the usual case: the atom's entries in shared memory */
+      for (int k = 0; k < cnt; k++) {
+        sj[wp][x - cnt + k] = v.slab_j[sb + k];
+        sd[wp][x - cnt + k] = v.slab_d2[sb + k];
+      }
+      __syncwarp();
+      for (int k = lane; k < m; k += 32) {
+        const float d2 = sd[wp][k];
+        const int j = sj[wp][k];
+        int rank = 0;
+        for (int b = 0; b < m; b++) {
+          const float db = sd[wp][b];
+          rank += (db < d2) || (db == d2 && sj[wp][b] < j);
+        }
+        v.nl_list[o + rank] = j;
+        v.nl_own[o + rank] = (int)g;
+      }
+      __syncwarp(); /* the buffer is read before the next atom fills it */
+      continue;
+    }
     for (int k = 0; k < cnt; k++) {
       v.nl_tmp[o + x - cnt + k] = v.slab_j[sb + k];
       v.nl_d2[o + x - cnt + k] = v.slab_d2[sb + k];
