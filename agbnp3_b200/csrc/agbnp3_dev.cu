@@ -121,6 +121,7 @@ struct View {
      are a compact cluster (identity until the first evaluation sets it) */
   const int *slot_atom, *atom_slot;
   int *slot_type; /* radius type by slot */
+  int *slot_hvcol; /* by slot: offset (hvslot[type] * AGB_NA) of the type's column of the shared tables */
   /* Verlet-skin reuse of the near list (skin > 0): candidates j > g within
      the near-list cutoff plus the skin, grouped by atom (CSR cand_off /
      cand_cnt), the positions they were built from, and per candidate the
@@ -150,6 +151,13 @@ struct View {
   /* Q4 tables as per-interval cubics in t = a/h - k, c0..c3 */
   const float4 *tabv_f;
   const double4 *tabv_d;
+  /* the FP32 tables whose descreener type has heavy atoms, as
+     [descreened type][heavy slot of the descreener type][AGB_NA], and the
+     heavy slot of each type (0 for a type only hydrogens have: its lookups
+     all fall on the zero record AGB_NA-1, the same in every table) */
+  const float4 *tabh_f;
+  const int *hvslot;
+  int nhv;
 };
 
 enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m */, DC_C0 = DC_L0 + 8 /* scratch */,
@@ -159,8 +167,10 @@ enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m
           candidates of the last build, builds so far */
        DC_REBUILD = DC_C0 + 8, DC_CLEN, DC_CTOT, DC_NCAND, DC_NBUILD,
        DC_SLABMAX /* near partners of the fullest overflowing (atom, cell) sub-slab */,
-       DC_N27 /* 27 N */ };
-#define DC_SIZE (DC_C0 + 15)
+       DC_N27 /* 27 N */,
+       DC_GBDQ /* next work item of the chain-rule pass (reset by k_agb_post) */,
+       DC_DESQ /* next half item of the descreening pass (reset by k_pack_sp) */ };
+#define DC_SIZE (DC_C0 + 17)
 
 /* record fields of a kept overlap, stored contiguously per record (12
    slots, three 4-wide vectors) */
@@ -1134,6 +1144,7 @@ __global__ void k_pack_geom(View v) {
     pa<R>(v, PA_ALPHA)[g] = R(C_KFC) / ((R)v.r[g] * (R)v.r[g]);
     pa<R>(v, PA_Q)[s] = (R)v.charge[g];
     v.slot_type[s] = v.rtype[g];
+    v.slot_hvcol[s] = v.hvslot[v.rtype[g]] * AGB_NA;
     v.acc_beta[g] = 0.0;
   }
 }
@@ -1144,6 +1155,7 @@ __global__ void k_pack_sp(View v) {
     R sp = (R)v.sp[g];
     pa<R>(v, PA_SP)[v.atom_slot[g]] = sp;
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) v.dc[DC_DESQ] = 0;
 }
 
 /* partner range of a work item: chunk w.w of nch of [p0, p1) */
@@ -1372,6 +1384,158 @@ __global__ void __launch_bounds__(ITILE / 2, DescBlocks<R>::v) k_descreen_t(View
   }
 }
 
+/* FP32 descreening with the heavy-descreener tables (View::tabh_f) in
+   shared memory: one block of DS_WARPS warps per SM.  Each warp takes half
+   an item (64 of its ITILE atoms, two per lane) from a device counter,
+   tests 32 partner tiles at a time against its atoms' bounding box (one
+   tile per lane) and stages each 32-slot tile in range itself, so after
+   the tables' copy no block barrier is needed. */
+#define DS_WARPS 32
+#define DS_GROUP 32 /* partners staged per warp: one 32-slot tile */
+
+/* the work unit of the c-th take from a device counter, for U units: the
+   takes run down the columns of a 148-row table of the units in order, so
+   that the warps of one SM, taking in a burst, get units far apart in the
+   list (neighbouring units cover neighbouring atoms and cost alike);
+   returns -1 for a take beyond the table and U + 1 for an empty cell */
+__device__ __forceinline__ int take_unit(int c, int U) {
+  const int K = (U + 147) / 148;
+  if (c >= 148 * K) return -1;
+  const int u = (c % 148) * K + c / 148;
+  return u < U ? u : U + 1;
+}
+template <bool SELF>
+__device__ __forceinline__ void desc_group_s(const Part4<float> *sp4, const PartW<float> *spw, int t0, int t1, int j0,
+                                             const int (&g)[2], const float (&xg)[2], const float (&yg)[2],
+                                             const float (&zg)[2], const float4 *ts, const int (&ro)[2],
+                                             float (&part)[2]) {
+#pragma unroll 4
+  for (int t = t0; t < t1; t++) {
+    const Part4<float> a = sp4[t];
+    const PartW<float> b = spw[t];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const float dx = a.x - xg[u], dy = a.y - yg[u], dz = a.z - zg[u];
+      const float xh = p_sqrt(dx * dx + dy * dy + dz * dz) * a.rh;
+      if (xh < float(AGB_NA - 1) && (!SELF || j0 + t != g[u])) {
+        const int k = (int)xh;
+        const float tt = xh - float(k);
+        const float4 c = ts[ro[u] + b.t + k];
+        part[u] += b.w * (c.x + tt * (c.y + tt * (c.z + tt * c.w)));
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(DS_WARPS * 32, 1) k_descreen_s(View v, const int4 *__restrict__ items, int nitems) {
+  extern __shared__ float4 ds_dyn[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  Part4<float> *sp4 = reinterpret_cast<Part4<float> *>(ds_dyn) + wid * DS_GROUP;
+  PartW<float> *spw = reinterpret_cast<PartW<float> *>(ds_dyn + DS_WARPS * DS_GROUP) + wid * DS_GROUP;
+  float4 *ts = ds_dyn + DS_WARPS * DS_GROUP + DS_WARPS * DS_GROUP / 2;
+  {
+    const int nrec = v.ntypes * v.nhv * AGB_NA;
+    for (int q = threadIdx.x; q < nrec; q += blockDim.x) ts[q] = __ldg(v.tabh_f + q);
+    __syncthreads();
+  }
+  const float *X = pa<float>(v, PA_X), *Y = pa<float>(v, PA_Y), *Z = pa<float>(v, PA_Z);
+  const float *RH = pa<float>(v, PA_RH), *W = pa<float>(v, PA_SP); /* the tables carry 1/R of the descreener */
+  const int nhv = v.nhv;
+  const int U = 2 * nitems;
+  int u = 0;
+  if (lane == 0) u = take_unit(atomicAdd(&v.dc[DC_DESQ], 1), U);
+  u = __shfl_sync(FULLMASK, u, 0);
+  while (u >= 0) {
+    if (u < U) {
+      const int4 w = items[u >> 1];
+      int g[2], ro[2];
+      bool act[2];
+      float xg[2], yg[2], zg[2];
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        g[k] = w.y + 64 * (u & 1) + lane + 32 * k;
+        act[k] = g[k] < w.z;
+        xg[k] = act[k] ? X[g[k]] : 0.f;
+        yg[k] = act[k] ? Y[g[k]] : 0.f;
+        zg[k] = act[k] ? Z[g[k]] : 0.f;
+        ro[k] = (act[k] ? v.slot_type[g[k]] * nhv : 0) * AGB_NA; /* the row of the atom's radius type */
+      }
+      if (__any_sync(FULLMASK, act[0])) {
+        /* this warp's bounding box */
+        float lx = INFINITY, ly = INFINITY, lz = INFINITY, hx = -INFINITY, hy = -INFINITY, hz = -INFINITY;
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+          if (act[k]) {
+            lx = fminf(lx, xg[k]);
+            ly = fminf(ly, yg[k]);
+            lz = fminf(lz, zg[k]);
+            hx = fmaxf(hx, xg[k]);
+            hy = fmaxf(hy, yg[k]);
+            hz = fmaxf(hz, zg[k]);
+          }
+        warp_minmax(lx, hx);
+        warp_minmax(ly, hy);
+        warp_minmax(lz, hz);
+        const float4 blo = make_float4(lx, ly, lz, 0.f), bhi = make_float4(hx, hy, hz, 0.f);
+        double acc[2] = {0.0, 0.0};
+        int p0 = v.inst_begin[w.x], c0, c1;
+        chunk_range(p0, p0 + v.inst_nheavy[w.x], w.w, c0, c1);
+        /* the chunk's 32-slot partner tiles, 32 tiles tested at once (one
+           per lane), then each tile in range staged and summed */
+        const int Tb = c0 >> 5, Te = (c1 - 1) >> 5;
+        for (int W0 = Tb; c1 > c0 && W0 <= Te; W0 += 32) {
+          const int T = W0 + lane;
+          unsigned mask = __ballot_sync(FULLMASK, T <= Te && tile_in_range(v.tbox, T, blo, bhi));
+          /* the tiles in range, the next one's partner loaded into registers
+             while the current one is summed */
+          int T1 = W0 + __ffs(mask) - 1, t0 = 0, n = 0;
+          Part4<float> a;
+          PartW<float> b;
+          const auto fetch = [&](int Tn) {
+            t0 = max(c0, 32 * Tn);
+            n = min(c1, 32 * Tn + 32) - t0;
+            if (lane < n) {
+              const int j = t0 + lane;
+              a.x = X[j];
+              a.y = Y[j];
+              a.z = Z[j];
+              a.rh = RH[j];
+              b.w = W[j];
+              b.t = v.slot_hvcol[j];
+            }
+          };
+          if (mask) fetch(T1);
+          while (mask) {
+            mask &= mask - 1;
+            const int c0t = t0, nt0 = n;
+            __syncwarp(); /* the previous tile's readers are done */
+            if (lane < nt0) {
+              sp4[lane] = a;
+              spw[lane] = b;
+            }
+            __syncwarp();
+            if (mask) fetch(W0 + __ffs(mask) - 1);
+            if (act[0]) {
+              float part[2] = {0.f, 0.f};
+              if (c0t < w.z && c0t + nt0 > w.y) /* the item's own atoms among the partners */
+                desc_group_s<true>(sp4, spw, 0, nt0, c0t, g, xg, yg, zg, ts, ro, part);
+              else
+                desc_group_s<false>(sp4, spw, 0, nt0, c0t, g, xg, yg, zg, ts, ro, part);
+              acc[0] += (double)part[0];
+              acc[1] += (double)part[1];
+            }
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+          if (act[k]) atomicAdd(&v.acc_beta[v.slot_atom[g[k]]], acc[k]);
+      }
+    }
+    if (lane == 0) u = take_unit(atomicAdd(&v.dc[DC_DESQ], 1), U);
+    u = __shfl_sync(FULLMASK, u, 0);
+  }
+}
+
 /* inverse Born radius, its filter, Born radius, vdW energy
    (agbnp3_cpu_simd_kernels.c:605, agbnp3.c:1174-1188, 1466-1487,
    agbnp3_utils.c:615-670) */
@@ -1487,6 +1651,7 @@ __global__ void k_agb_post(View v) {
     pa<R>(v, PA_ABRW)[v.atom_slot[g]] = (R)abrw;
     v.deru[g] = v.derv[g] = 0.0;
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) v.dc[DC_GBDQ] = 0;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -2639,6 +2804,8 @@ struct agb_dev {
   ncclComm_t comm;
   int nccl_err;
   int pair_order; /* 1: pair slots along a Hilbert curve, 0: identity */
+  size_t gbd_smem;  /* dynamic shared memory of the FP32 chain-rule pass with its tables, 0: tables from global memory */
+  size_t desc_smem; /* the same for the FP32 descreening pass */
   int order_ok;   /* the slot order is set for the current mode */
 };
 
@@ -2783,7 +2950,12 @@ static int build_items(agb_dev *s, int nch, int jb) {
     if (n > maxn) maxn = n;
   }
   if (nch <= 0) {
-    nch = (148 * 8 + ntiles - 1) / ntiles;
+    /* about 8 items per SM; with the shared-memory tables (one warp per
+       half item, 32 warps per SM) about 256, at most 32 chunks */
+    const bool sm = s->desc_smem > 0 && s->precision == AGB_PREC_MIXED;
+    const int target = sm ? 148 * 256 : 148 * 8;
+    nch = (target + ntiles - 1) / ntiles;
+    if (sm && nch > 32) nch = 32;
     if (nch > maxn / 512) nch = maxn / 512;
   }
   if (nch < 1) nch = 1;
@@ -3004,6 +3176,47 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     free(rt);
     UP(tabv_d, (const double4 *)tv, nrec, double4);
     UP(tabv_f, (const float4 *)fv, nrec, float4);
+    /* the tables of the descreener types that heavy atoms have (hydrogens
+       descreen nothing), compacted for the chain-rule pass's shared memory */
+    int *hv = (int *)calloc(nt > 0 ? nt : 1, sizeof(int));
+    int nhv = 0;
+    for (int I = 0; I < NI; I++)
+      for (int g = d->inst_begin[I]; g < d->inst_begin[I] + d->inst_nheavy[I]; g++) hv[d->rtype[g]] = 1;
+    for (int t = 0; t < nt; t++) hv[t] = hv[t] ? nhv++ : -1;
+    size_t nrh = (size_t)nt * (nhv > 0 ? nhv : 1) * AGB_NA;
+    float *fh = (float *)calloc(nrh * 4, sizeof(float));
+    for (int a = 0; a < nt; a++)
+      for (int b = 0; b < nt; b++)
+        if (hv[b] >= 0)
+          memcpy(fh + 4 * ((size_t)(a * nhv + hv[b]) * AGB_NA), fv + 4 * ((size_t)(a * nt + b) * AGB_NA),
+                 sizeof(float) * 4 * AGB_NA);
+    for (int t = 0; t < nt; t++) hv[t] = hv[t] < 0 ? 0 : hv[t];
+    v.nhv = nhv;
+    {
+      /* the chain-rule pass holds these tables in shared memory when they
+         fit beside its 16 warps' j tiles */
+      int smax = 0;
+      CK(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, d->device));
+      const size_t need = sizeof(float4) * ((size_t)16 * 4 * 32 + (size_t)nt * nhv * AGB_NA);
+      const char *e = getenv("AGBNP3_GBD_SMEM");
+      s->gbd_smem = 0;
+      if (nhv > 0 && need <= (size_t)smax && (!e || atoi(e) != 0)) {
+        CK(cudaFuncSetAttribute(k_gbders_x2<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+        CK(cudaFuncSetAttribute(k_gbders_x2<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+        s->gbd_smem = need;
+      }
+      const size_t dneed = sizeof(float4) * ((size_t)DS_WARPS * DS_GROUP * 3 / 2 + (size_t)nt * nhv * AGB_NA);
+      const char *e2 = getenv("AGBNP3_DESC_SMEM");
+      s->desc_smem = 0;
+      if (nhv > 0 && dneed <= (size_t)smax && (!e2 || atoi(e2) != 0)) {
+        CK(cudaFuncSetAttribute(k_descreen_s, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dneed));
+        s->desc_smem = dneed;
+      }
+    }
+    UP(tabh_f, (const float4 *)fh, nrh, float4);
+    UP(hvslot, hv, nt > 0 ? nt : 1, int);
+    free(fh);
+    free(hv);
     free(tv);
     free(fv);
   }
@@ -3101,6 +3314,7 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
     UP(atom_slot, id, N, int);
     free(id);
     DALLOC(v.slot_type, N, int);
+    DALLOC(v.slot_hvcol, N, int);
     s->h_ext_of = (int *)malloc(sizeof(int) * N);
     memcpy(s->h_ext_of, d->ext_of, sizeof(int) * N);
     const char *po = getenv("AGBNP3_PAIR_ORDER");
@@ -3405,6 +3619,29 @@ static void launch_ws(agb_dev *s, const View &v, cudaStream_t stream) {
   AGB_LAUNCH(k_ws_free<R>, sym_grid(s->nws), 128, stream, v);
 }
 
+/* the FP32 chain-rule pass: with the heavy-descreener tables in shared
+   memory when they fit (one 16-warp block per SM), else from global memory */
+static void launch_gbders_x2(agb_dev *s, cudaStream_t st) {
+  const View &v = s->v;
+  if (s->gbd_smem > 0) {
+    /* a block on every SM, of as many warps (up to 16) as the items fill;
+       the warps take the items in turn from a counter */
+    int grid = s->n_gbd > 148 ? 148 : (s->n_gbd < 1 ? 1 : s->n_gbd);
+    int nw = (s->n_gbd + 147) / 148;
+    nw = nw > 16 ? 16 : (nw < 1 ? 1 : nw);
+    if (s->compat)
+      k_gbders_x2<true, true><<<grid, nw * 32, s->gbd_smem, st>>>(v, s->items_gbd, s->n_gbd);
+    else
+      k_gbders_x2<false, true><<<grid, nw * 32, s->gbd_smem, st>>>(v, s->items_gbd, s->n_gbd);
+  } else {
+    const size_t shb = sizeof(float4) * 4 * 4 * 32;
+    if (s->compat)
+      k_gbders_x2<true, false><<<sym_grid(s->n_gbd), 128, shb, st>>>(v, s->items_gbd, s->n_gbd);
+    else
+      k_gbders_x2<false, false><<<sym_grid(s->n_gbd), 128, shb, st>>>(v, s->items_gbd, s->n_gbd);
+  }
+}
+
 static void stage_mark(agb_dev *s, int k) {
   if (s->timing) cudaEventRecord(s->ev[k], s->st);
 }
@@ -3528,7 +3765,18 @@ static void launch_all(agb_dev *s, int seg = -1) {
     nl += 4 + AGB_SCAN_LAUNCHES;
   }
   int dgrid = s->nitems < 148 * 32 ? s->nitems : 148 * 32; /* 64-thread descreening blocks */
-  AGB_LAUNCH(k_descreen_t<R>, dgrid > 0 ? dgrid : 1, ITILE / 2, st, v, s->items, s->nitems, s->nch);
+  if (sizeof(R) == 4 && s->desc_smem > 0) {
+    /* a block on every SM, of as many warps as the half items fill (the
+       warps take them in turn from a counter: more warps than half items
+       per SM would leave the later SMs without work) */
+    const int units = 2 * s->nitems;
+    int grid = units > 148 ? 148 : (units < 1 ? 1 : units);
+    int nw = (units + 147) / 148;
+    nw = nw > DS_WARPS ? DS_WARPS : (nw < 1 ? 1 : nw);
+    k_descreen_s<<<grid, nw * 32, s->desc_smem, st>>>(v, s->items, s->nitems);
+  } else {
+    AGB_LAUNCH(k_descreen_t<R>, dgrid > 0 ? dgrid : 1, ITILE / 2, st, v, s->items, s->nitems, s->nch);
+  }
   nl += 1;
   }
   const int pgrid = s->nitems < 148 * 16 ? (s->nitems > 0 ? s->nitems : 1) : 148 * 16;
@@ -3552,10 +3800,8 @@ static void launch_all(agb_dev *s, int seg = -1) {
   stage_mark(s, 6);
   if (s->tiled_pairs)
     AGB_LAUNCH(k_gbders_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
-  else if (sizeof(R) == 4 && !s->scalar_pairs && s->compat)
-    AGB_LAUNCH(k_gbders_x2<true>, sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
   else if (sizeof(R) == 4 && !s->scalar_pairs)
-    AGB_LAUNCH(k_gbders_x2<false>, sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
+    launch_gbders_x2(s, st);
   else if (s->compat)
     AGB_LAUNCH((k_gbders_sym<R, true>), sym_grid(s->n_gbd), 128, st, v, s->items_gbd, s->n_gbd);
   else

@@ -212,12 +212,12 @@ __device__ __forceinline__ float2 clamp_na2(float2 x) {
   return make_float2(fminf(x.x, float(AGB_NA - 1)), fminf(x.y, float(AGB_NA - 1)));
 }
 
-/* Q4/R and its derivative in t at interval record idx (one 16-byte load;
-   the derivative forms of spline_d: REF the reference's convention, else
-   the exact derivative of the cubic) */
-template <bool REF>
+/* Q4/R and its derivative in t at interval record idx (one 16-byte load,
+   from shared memory when SMEM; the derivative forms of spline_d: REF the
+   reference's convention, else the exact derivative of the cubic) */
+template <bool REF, bool SMEM>
 __device__ __forceinline__ void q4_rec(const float4 *__restrict__ tv, int idx, float t, float &q, float &fp) {
-  const float4 c = __ldg(tv + idx);
+  const float4 c = SMEM ? tv[idx] : __ldg(tv + idx);
   q = fmaf(t, fmaf(t, fmaf(t, c.w, c.z), c.y), c.x);
   const float d0 = REF ? fmaf(2.f, c.w, fmaf(2.f / 3.f, c.z, c.y)) : c.y;
   const float d2 = REF ? -fmaf(3.f, c.w, 2.f * c.z) : 3.f * c.w;
@@ -249,7 +249,7 @@ struct GxJ {
   float U, V, fx, fy, fz, vx, vy, vz;
 };
 
-template <int MODE, bool REF>
+template <int MODE, bool REF, bool SMEM>
 __device__ __forceinline__ void gbd_tile_x2(const GxI &I, GxP &P, GxJ &J, const float4 (*sj)[32], int lane, int j0,
                                             const float4 *__restrict__ tv) {
   constexpr bool TWO = MODE != GBD_HX; /* both descreening directions possible */
@@ -313,8 +313,8 @@ __device__ __forceinline__ void gbd_tile_x2(const GxI &I, GxP &P, GxJ &J, const 
       float2 fk1;
       const float2 t1 = floor_frac2(clamp_na2(xh1), fk1);
       float2 q1, fp1;
-      q4_rec<REF>(tv, __float_as_int(fk1.x) + I.o1[2 * p] + o1j, t1.x, q1.x, fp1.x);
-      q4_rec<REF>(tv, __float_as_int(fk1.y) + I.o1[2 * p + 1] + o1j, t1.y, q1.y, fp1.y);
+      q4_rec<REF, SMEM>(tv, __float_as_int(fk1.x) + I.o1[2 * p] + o1j, t1.x, q1.x, fp1.x);
+      q4_rec<REF, SMEM>(tv, __float_as_int(fk1.y) + I.o1[2 * p + 1] + o1j, t1.y, q1.y, fp1.y);
       P.U[p] = fma2(jq2, q1, P.U[p]);
       P.V[p] = fma2(jab, q1, P.V[p]);
       const float2 dqs1 = mul2(fp1, I.rs[p]);
@@ -323,8 +323,8 @@ __device__ __forceinline__ void gbd_tile_x2(const GxI &I, GxP &P, GxJ &J, const 
         float2 fk2;
         const float2 t2 = floor_frac2(clamp_na2(xh2), fk2);
         float2 q2, fp2;
-        q4_rec<REF>(tv, __float_as_int(fk2.x) + I.o2[2 * p] + o2j, t2.x, q2.x, fp2.x);
-        q4_rec<REF>(tv, __float_as_int(fk2.y) + I.o2[2 * p + 1] + o2j, t2.y, q2.y, fp2.y);
+        q4_rec<REF, SMEM>(tv, __float_as_int(fk2.x) + I.o2[2 * p] + o2j, t2.x, q2.x, fp2.x);
+        q4_rec<REF, SMEM>(tv, __float_as_int(fk2.y) + I.o2[2 * p + 1] + o2j, t2.y, q2.y, fp2.y);
         J.U = fmaf(I.q2[p].x, q2.x, fmaf(I.q2[p].y, q2.y, J.U));
         J.V = fmaf(I.ab[p].x, q2.x, fmaf(I.ab[p].y, q2.y, J.V));
         const float2 dqs2 = mul2(fp2, jrs);
@@ -357,20 +357,52 @@ __device__ __forceinline__ void gbd_tile_x2(const GxI &I, GxP &P, GxJ &J, const 
   }
 }
 
-/* four resident blocks per SM at 128 registers (ptxas spills about 50
-   bytes per thread); three blocks at 162 registers without spills
-   measured 1 % slower */
-template <bool REF>
-__global__ void __launch_bounds__(128, 4) k_gbders_x2(View v, const int4 *__restrict__ items, int nitems) {
-  __shared__ float4 sjt[4][4][32];
+/* GBD_NW warps per block.  Tables in global memory (SMEM false): four
+   resident blocks of 4 warps per SM at 128 registers (ptxas spills about 50
+   bytes per thread; three blocks at 162 registers without spills measured
+   1 % slower), one item per warp in grid order.  SMEM: the heavy-descreener
+   tables (View::tabh_f) copied into shared memory by one block of 16 warps
+   per SM, whose warps take items from a device counter. */
+template <bool SMEM>
+struct GbdNW {
+  static constexpr int v = SMEM ? 16 : 4;
+};
+template <bool REF, bool SMEM>
+__global__ void __launch_bounds__(GbdNW<SMEM>::v * 32, SMEM ? 1 : 4) k_gbders_x2(View v, const int4 *__restrict__ items,
+                                                                                   int nitems) {
+  constexpr int NW = GbdNW<SMEM>::v;
+  extern __shared__ float4 gbd_dyn[];
+  float4(*sjt)[4][32] = reinterpret_cast<float4(*)[4][32]>(gbd_dyn); /* [NW][4][32] */
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const float *X = pa<float>(v, PA_X), *Y = pa<float>(v, PA_Y), *Z = pa<float>(v, PA_Z);
   const float *RH = pa<float>(v, PA_RH), *SP = pa<float>(v, PA_SP);
   const float *Q2 = pa<float>(v, PA_Q2AB), *AB = pa<float>(v, PA_ABRW);
-  const float4 *tv = v.tabv_f;
   const int nt = v.ntypes;
+  const float4 *tv = v.tabv_f;
+  /* table offsets: (descreened type, descreener type) is record row
+     d * nt + e of the full tables, d * nhv + hvslot[e] of the shared copy */
+  const int ncol = SMEM ? v.nhv : nt;
+  if (SMEM) {
+    float4 *ts = gbd_dyn + NW * 4 * 32;
+    const int nrec = nt * v.nhv * AGB_NA;
+    for (int q = threadIdx.x; q < nrec; q += blockDim.x) ts[q] = __ldg(v.tabh_f + q);
+    tv = ts;
+    __syncthreads();
+  }
   const double f4p = 1.0 / (4.0 * C_PI);
-  for (int it = blockIdx.x * 4 + wp; it < nitems; it += gridDim.x * 4) {
+  /* SMEM: items from the counter, spread over the list by take_unit (-1:
+     none left, nitems + 1: an empty cell of its table) */
+  int it = blockIdx.x * NW + wp;
+  if (SMEM) {
+    if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_GBDQ], 1), nitems);
+    it = __shfl_sync(FULLMASK, it, 0);
+  }
+  while (SMEM ? it >= 0 : it < nitems) {
+    if (SMEM && it >= nitems) {
+      if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_GBDQ], 1), nitems);
+      it = __shfl_sync(FULLMASK, it, 0);
+      continue;
+    }
     const int4 w = items[it];
     const int a0 = v.inst_begin[w.x], hh = a0 + v.inst_nheavy[w.x], a1 = v.inst_begin[w.x + 1];
     const double kg = f4p * v.inst_df[w.x];
@@ -395,8 +427,8 @@ __global__ void __launch_bounds__(128, 4) k_gbders_x2(View v, const int4 *__rest
         t[h][4] = ok ? rh * SP[i] : 0.f;
         t[h][5] = ok ? Q2[i] : 0.f;
         t[h][6] = ok ? AB[i] : 0.f;
-        I.o1[u] = ti * AGB_NA - X2_TWO23_BITS;
-        I.o2[u] = ti * nt * AGB_NA - X2_TWO23_BITS;
+        I.o1[u] = (SMEM ? v.hvslot[ti] : ti) * AGB_NA - X2_TWO23_BITS;
+        I.o2[u] = ti * ncol * AGB_NA - X2_TWO23_BITS;
       }
       I.nx[p] = make_float2(t[0][0], t[1][0]);
       I.ny[p] = make_float2(t[0][1], t[1][1]);
@@ -420,18 +452,19 @@ __global__ void __launch_bounds__(128, 4) k_gbders_x2(View v, const int4 *__rest
       sjt[wp][0][lane] = make_float4(xj, xj, yj, yj);
       sjt[wp][1][lane] = make_float4(zj, zj, rhj, rhj);
       sjt[wp][2][lane] = make_float4(rsj, rsj, q2j, q2j);
-      sjt[wp][3][lane] = make_float4(abj, abj, __int_as_float(tj * nt * AGB_NA), __int_as_float(tj * AGB_NA));
+      sjt[wp][3][lane] = make_float4(abj, abj, __int_as_float(tj * ncol * AGB_NA),
+                                     __int_as_float((SMEM ? v.hvslot[tj] : tj) * AGB_NA));
       __syncwarp();
       GxJ J;
       J.U = J.V = J.fx = J.fy = J.fz = J.vx = J.vy = J.vz = 0.f;
       /* warp-uniform tile class */
       const bool interior = iheavy && j0 >= w.y + 64 * AX_NP;
       if (interior && j0 + 32 <= hh)
-        gbd_tile_x2<GBD_HH, REF>(I, P, J, sjt[wp], lane, j0, tv);
+        gbd_tile_x2<GBD_HH, REF, SMEM>(I, P, J, sjt[wp], lane, j0, tv);
       else if (interior && j0 >= hh && j0 + 32 <= a1)
-        gbd_tile_x2<GBD_HX, REF>(I, P, J, sjt[wp], lane, j0, tv);
+        gbd_tile_x2<GBD_HX, REF, SMEM>(I, P, J, sjt[wp], lane, j0, tv);
       else
-        gbd_tile_x2<GBD_GEN, REF>(I, P, J, sjt[wp], lane, j0, tv);
+        gbd_tile_x2<GBD_GEN, REF, SMEM>(I, P, J, sjt[wp], lane, j0, tv);
       if (vj) {
         const int ja = v.slot_atom[j];
         atomicAdd(&v.g_gb[3 * ja], kg * (double)J.fx);
@@ -462,6 +495,12 @@ __global__ void __launch_bounds__(128, 4) k_gbders_x2(View v, const int4 *__rest
         atomicAdd(&v.deru[i], (double)lo_hi(P.U[p], h));
         atomicAdd(&v.derv[i], (double)lo_hi(P.V[p], h));
       }
+    }
+    if (SMEM) {
+      if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_GBDQ], 1), nitems);
+      it = __shfl_sync(FULLMASK, it, 0);
+    } else {
+      it += gridDim.x * NW;
     }
   }
 }

@@ -480,6 +480,50 @@ def test_one_sided_pair_kernels(engine, monkeypatch, prec):
         base.close()
 
 
+@pytest.mark.parametrize("gbd,desc", [("0", "0"), ("0", "1"), ("1", "0")],
+                         ids=["both_global", "chain_rule_global", "descreening_global"])
+def test_table_placement(engine, monkeypatch, gbd, desc):
+    """The FP32 descreening and chain-rule passes read their Q4 tables from
+    shared memory by default (the tables of the heavy descreener types,
+    copied once per SM) and from global memory with AGBNP3_DESC_SMEM=0 /
+    AGBNP3_GBD_SMEM=0: every placement against the oracle, and against the
+    default one to within float summation order."""
+    s, _ = load_golden("globule2000_hbmix")
+    q = O.oracle_eval(s)
+    base = A.Instance(s, precision=A.PREC_MIXED)
+    monkeypatch.setenv("AGBNP3_GBD_SMEM", gbd)
+    monkeypatch.setenv("AGBNP3_DESC_SMEM", desc)
+    inst = A.Instance(s, precision=A.PREC_MIXED)
+    try:
+        r, b = inst.ener(), base.ener()
+        check_vs_oracle(r, q, A.PREC_MIXED, f"gbd={gbd} desc={desc}")
+        for k in ENERGY_KEYS:
+            assert abs(r[k] - b[k]) <= 1e-6 * max(abs(b[k]), 1.0), (k, r[k], b[k])
+        for k in ("br", "dgbdr", "dvwdr"):
+            assert rms_rel(r[k], b[k]) <= 1e-5, (k, rms_rel(r[k], b[k]))
+    finally:
+        inst.close()
+        base.close()
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
+def test_many_radius_types(engine, prec):
+    """A 2,000-atom globule whose heavy atoms carry twelve distinct radii:
+    the heavy-descreener tables (13 x 12 tables of 8 KB) do not fit in shared
+    memory, so the FP32 passes fall back to tables in global memory; energies
+    and forces against the oracle."""
+    s = A.make_globule(2000, 5)
+    heavy = np.setdiff1d(np.arange(s.natoms), s.ihydrogen)
+    s.r = s.r.copy()
+    s.r[heavy] = np.random.default_rng(3).choice(np.linspace(1.5, 2.05, 12), size=heavy.size)
+    q = O.oracle_eval(s)
+    inst = A.Instance(s, precision=prec)
+    try:
+        check_vs_oracle(inst.ener(), q, prec, "12 heavy radii")
+    finally:
+        inst.close()
+
+
 @pytest.mark.parametrize("prec", [A.PREC_FP64, A.PREC_MIXED], ids=["fp64", "mixed"])
 def test_pair_slot_order(engine, prec):
     """Hilbert-ordered pair slots (the default) against the internal order:
