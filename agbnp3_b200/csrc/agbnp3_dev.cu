@@ -169,8 +169,9 @@ enum { DC_N = 0, DC_NB, DC_NWS, DC_NL, DC_ERR, DC_L0 /* DC_L0+m: kept of order m
        DC_SLABMAX /* near partners of the fullest overflowing (atom, cell) sub-slab */,
        DC_N27 /* 27 N */,
        DC_GBDQ /* next work item of the chain-rule pass (reset by k_agb_post) */,
-       DC_DESQ /* next half item of the descreening pass (reset by k_pack_sp) */ };
-#define DC_SIZE (DC_C0 + 17)
+       DC_DESQ /* next half item of the descreening pass (reset by k_pack_sp) */,
+       DC_AGBQ /* next work item of the GB pair pass (reset by k_born) */ };
+#define DC_SIZE (DC_C0 + 18)
 
 /* record fields of a kept overlap, stored contiguously per record (12
    slots, three 4-wide vectors) */
@@ -1565,6 +1566,7 @@ __global__ void k_born(View v) {
     pa<R>(v, PA_B)[v.atom_slot[g]] = (R)b;
     pa<R>(v, PA_BINV)[v.atom_slot[g]] = (R)bf;
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) v.dc[DC_AGBQ] = 0;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -3619,27 +3621,23 @@ static void launch_ws(agb_dev *s, const View &v, cudaStream_t stream) {
   AGB_LAUNCH(k_ws_free<R>, sym_grid(s->nws), 128, stream, v);
 }
 
-/* the FP32 chain-rule pass: with the heavy-descreener tables in shared
-   memory when they fit (one 16-warp block per SM), else from global memory */
+/* the FP32 chain-rule pass: a block on every SM, of as many warps (up to
+   16) as the items fill, with the heavy-descreener tables in shared memory
+   when they fit, else read from global memory */
 static void launch_gbders_x2(agb_dev *s, cudaStream_t st) {
   const View &v = s->v;
-  if (s->gbd_smem > 0) {
-    /* a block on every SM, of as many warps (up to 16) as the items fill;
-       the warps take the items in turn from a counter */
-    int grid = s->n_gbd > 148 ? 148 : (s->n_gbd < 1 ? 1 : s->n_gbd);
-    int nw = (s->n_gbd + 147) / 148;
-    nw = nw > 16 ? 16 : (nw < 1 ? 1 : nw);
-    if (s->compat)
-      k_gbders_x2<true, true><<<grid, nw * 32, s->gbd_smem, st>>>(v, s->items_gbd, s->n_gbd);
-    else
-      k_gbders_x2<false, true><<<grid, nw * 32, s->gbd_smem, st>>>(v, s->items_gbd, s->n_gbd);
-  } else {
-    const size_t shb = sizeof(float4) * 4 * 4 * 32;
-    if (s->compat)
-      k_gbders_x2<true, false><<<sym_grid(s->n_gbd), 128, shb, st>>>(v, s->items_gbd, s->n_gbd);
-    else
-      k_gbders_x2<false, false><<<sym_grid(s->n_gbd), 128, shb, st>>>(v, s->items_gbd, s->n_gbd);
-  }
+  const int grid = s->n_gbd > 148 ? 148 : (s->n_gbd < 1 ? 1 : s->n_gbd);
+  int nw = (s->n_gbd + 147) / 148;
+  nw = nw > 16 ? 16 : (nw < 1 ? 1 : nw);
+  const size_t shb = s->gbd_smem > 0 ? s->gbd_smem : sizeof(float4) * 16 * 4 * 32;
+  if (s->gbd_smem > 0 && s->compat)
+    k_gbders_x2<true, true><<<grid, nw * 32, shb, st>>>(v, s->items_gbd, s->n_gbd);
+  else if (s->gbd_smem > 0)
+    k_gbders_x2<false, true><<<grid, nw * 32, shb, st>>>(v, s->items_gbd, s->n_gbd);
+  else if (s->compat)
+    k_gbders_x2<true, false><<<grid, nw * 32, shb, st>>>(v, s->items_gbd, s->n_gbd);
+  else
+    k_gbders_x2<false, false><<<grid, nw * 32, shb, st>>>(v, s->items_gbd, s->n_gbd);
 }
 
 static void stage_mark(agb_dev *s, int k) {
@@ -3787,8 +3785,13 @@ static void launch_all(agb_dev *s, int seg = -1) {
   stage_mark(s, 5);
   if (s->tiled_pairs)
     AGB_LAUNCH(k_agb_t<R>, pgrid, ITILE, st, v, s->items, s->nitems, s->nch);
-  else if (sizeof(R) == 4 && !s->scalar_pairs)
-    AGB_LAUNCH(k_agb_x2, sym_grid(s->n_agb), 128, st, v, s->items_agb, s->n_agb);
+  else if (sizeof(R) == 4 && !s->scalar_pairs) {
+    /* a block on every SM, of as many warps (up to 16) as the items fill */
+    const int grid = s->n_agb > 148 ? 148 : (s->n_agb < 1 ? 1 : s->n_agb);
+    int nw = (s->n_agb + 147) / 148;
+    nw = nw > 16 ? 16 : (nw < 1 ? 1 : nw);
+    AGB_LAUNCH(k_agb_x2, grid, nw * 32, st, v, s->items_agb, s->n_agb);
+  }
   else
     AGB_LAUNCH(k_agb_sym<R>, sym_grid(s->n_agb), 128, st, v, s->items_agb, s->n_agb);
   nl += 1;

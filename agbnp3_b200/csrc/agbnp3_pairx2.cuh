@@ -119,13 +119,23 @@ __device__ __forceinline__ void agb_tile_x2(const AxI &I, AxP &P, AxJ &J, const 
 
 /* 116 registers: four resident blocks per SM (five, at 96 registers with
    spills, measured 2 % slower) */
-__global__ void __launch_bounds__(128, 4) k_agb_x2(View v, const int4 *__restrict__ items, int nitems) {
-  __shared__ float4 sjt[4][3][32];
+/* one block of up to 16 warps per SM, whose warps take the items from a
+   device counter (spread over the list by take_unit): 2-6 % faster than
+   four 4-warp blocks per SM taking items in grid order */
+__global__ void __launch_bounds__(512, 1) k_agb_x2(View v, const int4 *__restrict__ items, int nitems) {
+  __shared__ float4 sjt[16][3][32];
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const float *X = pa<float>(v, PA_X), *Y = pa<float>(v, PA_Y), *Z = pa<float>(v, PA_Z);
   const float *Q = pa<float>(v, PA_Q), *Bv = pa<float>(v, PA_B), *BI = pa<float>(v, PA_BINV);
   const size_t N = v.natoms;
-  for (int it = blockIdx.x * 4 + wp; it < nitems; it += gridDim.x * 4) {
+  int it = 0;
+  if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_AGBQ], 1), nitems);
+  it = __shfl_sync(FULLMASK, it, 0);
+  for (; it >= 0; it = __shfl_sync(FULLMASK, it, 0)) {
+    if (it >= nitems) { /* an empty cell of take_unit's table */
+      if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_AGBQ], 1), nitems);
+      continue;
+    }
     const int4 w = items[it]; /* instance, first atom of the i block, first atom of the j run, j tiles */
     const int a1 = v.inst_begin[w.x + 1];
     const double w2 = 2.0 * v.inst_df[w.x];
@@ -192,6 +202,7 @@ __global__ void __launch_bounds__(128, 4) k_agb_x2(View v, const int4 *__restric
       atomicAdd(&v.g_gb[3 * i + 2], w2 * (double)lo_hi(P.gz[p], h));
       atomicAdd(&v.dera[i], (double)lo_hi(P.at[p], h));
     }
+    if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_AGBQ], 1), nitems);
   }
 }
 
@@ -357,20 +368,14 @@ __device__ __forceinline__ void gbd_tile_x2(const GxI &I, GxP &P, GxJ &J, const 
   }
 }
 
-/* GBD_NW warps per block.  Tables in global memory (SMEM false): four
-   resident blocks of 4 warps per SM at 128 registers (ptxas spills about 50
-   bytes per thread; three blocks at 162 registers without spills measured
-   1 % slower), one item per warp in grid order.  SMEM: the heavy-descreener
-   tables (View::tabh_f) copied into shared memory by one block of 16 warps
-   per SM, whose warps take items from a device counter. */
-template <bool SMEM>
-struct GbdNW {
-  static constexpr int v = SMEM ? 16 : 4;
-};
+/* one block of up to 16 warps per SM, whose warps take the items from a
+   device counter (spread over the list by take_unit).  SMEM: the Q4 tables
+   of the heavy descreener types (View::tabh_f) are copied into shared
+   memory first (no register spills then; with the tables in global memory
+   ptxas spills a few dozen bytes per thread at the 128-register cap). */
 template <bool REF, bool SMEM>
-__global__ void __launch_bounds__(GbdNW<SMEM>::v * 32, SMEM ? 1 : 4) k_gbders_x2(View v, const int4 *__restrict__ items,
-                                                                                   int nitems) {
-  constexpr int NW = GbdNW<SMEM>::v;
+__global__ void __launch_bounds__(512, 1) k_gbders_x2(View v, const int4 *__restrict__ items, int nitems) {
+  constexpr int NW = 16;
   extern __shared__ float4 gbd_dyn[];
   float4(*sjt)[4][32] = reinterpret_cast<float4(*)[4][32]>(gbd_dyn); /* [NW][4][32] */
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
@@ -390,17 +395,12 @@ __global__ void __launch_bounds__(GbdNW<SMEM>::v * 32, SMEM ? 1 : 4) k_gbders_x2
     __syncthreads();
   }
   const double f4p = 1.0 / (4.0 * C_PI);
-  /* SMEM: items from the counter, spread over the list by take_unit (-1:
-     none left, nitems + 1: an empty cell of its table) */
-  int it = blockIdx.x * NW + wp;
-  if (SMEM) {
-    if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_GBDQ], 1), nitems);
-    it = __shfl_sync(FULLMASK, it, 0);
-  }
-  while (SMEM ? it >= 0 : it < nitems) {
-    if (SMEM && it >= nitems) {
+  int it = 0;
+  if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_GBDQ], 1), nitems);
+  it = __shfl_sync(FULLMASK, it, 0);
+  for (; it >= 0; it = __shfl_sync(FULLMASK, it, 0)) {
+    if (it >= nitems) { /* an empty cell of take_unit's table */
       if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_GBDQ], 1), nitems);
-      it = __shfl_sync(FULLMASK, it, 0);
       continue;
     }
     const int4 w = items[it];
@@ -496,11 +496,6 @@ __global__ void __launch_bounds__(GbdNW<SMEM>::v * 32, SMEM ? 1 : 4) k_gbders_x2
         atomicAdd(&v.derv[i], (double)lo_hi(P.V[p], h));
       }
     }
-    if (SMEM) {
-      if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_GBDQ], 1), nitems);
-      it = __shfl_sync(FULLMASK, it, 0);
-    } else {
-      it += gridDim.x * NW;
-    }
+    if (lane == 0) it = take_unit(atomicAdd(&v.dc[DC_GBDQ], 1), nitems);
   }
 }

@@ -291,7 +291,7 @@ def pair_roofline(natoms, nheavy, stage_ms, peaks):
                                  "fp32_frac": tot_fl / (tot_ms * 1e-3) / 1e12 / peaks["fp32_tflops"]}
     dom = max(work, key=lambda k: stages[k]["ms"])
     d = stages[dom]
-    kern = {"gbders": "k_gbders_x2", "agb": "k_agb_x2", "invb": "k_descreen_t"}[dom]  # FP32 (chosen mode) kernels
+    kern = {"gbders": "k_gbders_x2", "agb": "k_agb_x2", "invb": "k_descreen_s"}[dom]  # FP32 (chosen mode) kernels
     tr = load_traffic(natoms)
     hits = [v for n, v in tr["kernels"].items() if n == kern or n.startswith(kern + "<")] if tr else []
     traffic = hits[0]["dram_bytes_per_launch"] if len(hits) == 1 else None
