@@ -112,6 +112,7 @@ struct View {
   double *eatom;                      /* [7][natoms] */
   double *ews;                        /* [nws] */
   void *wpos, *wdpos;                 /* R[3*nws], R[36*nws] */
+  void *tdat;                         /* TdAtom<R>[natoms]: what the tree-derivative pass reads per parent */
   double *wsp;                        /* [nws] */
   double *o_sp, *o_br, *o_sa, *o_gb, *o_gv, *o_gc, *o_gh;
   int nbuckets;
@@ -2115,20 +2116,48 @@ __global__ void __launch_bounds__(128) k_gbders_sym(View v, const int4 *__restri
 
 /* U_i, V_i normalised by the atomic volume and the surface-area effective
    gammas (agbnp3_cpu_simd_kernels.c:861-874) */
+/* the per-atom values the tree-derivative pass reads for each parent of a
+   record, in one record per atom (three or five 16-byte loads instead of
+   nine scattered ones): U_i and V_i over the self volume, the cavity, vdW
+   and GB weights gammap, dervs, derus, the Gaussian exponent, 1/R and the
+   position.  The HB weight derh comes from the water-site stage, which may
+   still run beside this kernel, and is read on its own. */
+template <typename R>
+struct alignas(16) TdAtom {
+  double du, dv;
+  R wc, wv, wb, ga, gr, x, y, z;
+};
+static_assert(sizeof(TdAtom<double>) <= 80, "tdat holds 80 bytes per atom");
+
+template <typename R>
 __global__ void k_gbders_post(View v) {
   AGB_GRID_STRIDE(g, v.natoms) {
     int I = v.inst_of[g];
+    double du = 0.0, dv = 0.0, dvs = 0.0, dus = 0.0;
     if (g < v.inst_begin[I] + v.inst_nheavy[I]) {
       const double f4p = 1.0 / (4.0 * C_PI);
       double vol = v.vols[g];
-      double du = v.deru[g] / vol, dv = v.derv[g] / vol;
-      v.deru[g] = du;
-      v.derv[g] = dv;
-      v.dervs[g] = f4p * v.psvol[g] * dv;
-      v.derus[g] = v.inst_df[I] * f4p * v.psvol[g] * du;
-    } else {
-      v.deru[g] = v.derv[g] = v.dervs[g] = v.derus[g] = 0.0;
+      du = v.deru[g] / vol;
+      dv = v.derv[g] / vol;
+      dvs = f4p * v.psvol[g] * dv;
+      dus = v.inst_df[I] * f4p * v.psvol[g] * du;
     }
+    v.deru[g] = du;
+    v.derv[g] = dv;
+    v.dervs[g] = dvs;
+    v.derus[g] = dus;
+    TdAtom<R> t;
+    t.du = du;
+    t.dv = dv;
+    t.wc = (R)v.gammap[g];
+    t.wv = (R)dvs;
+    t.wb = (R)dus;
+    t.ga = atom_alpha<R>(v, g);
+    t.gr = atom_rinv<R>(v, g);
+    t.x = px<R>(v, g);
+    t.y = py<R>(v, g);
+    t.z = pz<R>(v, g);
+    ((TdAtom<R> *)v.tdat)[g] = t;
   }
 }
 
@@ -2592,17 +2621,18 @@ __global__ void __launch_bounds__(256) k_tree_ders(View v) {
       double du = 0.0, dv = 0.0, dh = 0.0;
 #pragma unroll
       for (int k = 0; k < M; k++) {
-        int a = par[k];
-        du += v.deru[a];
-        dv += v.derv[a];
+        const int a = par[k];
+        const TdAtom<R> t = ((const TdAtom<R> *)v.tdat)[a];
+        du += t.du;
+        dv += t.dv;
         dh += v.derh[a];
-        wc[k] = (R)(sgn * v.gammap[a]);
-        wv[k] = (R)(sgn * v.dervs[a]);
-        wb[k] = (R)(sgn * v.derus[a]);
-        ga[k] = atom_alpha<R>(v, a);
-        gr[k] = atom_rinv<R>(v, a); /* 1/R */
+        wc[k] = R(sgn) * t.wc;
+        wv[k] = R(sgn) * t.wv;
+        wb[k] = R(sgn) * t.wb;
+        ga[k] = t.ga;
+        gr[k] = t.gr; /* 1/R */
         R u1 = ga[k] * gvol;
-        R xk[3] = {px<R>(v, a) - cx, py<R>(v, a) - cy, pz<R>(v, a) - cz};
+        R xk[3] = {t.x - cx, t.y - cy, t.z - cz};
         R d2 = R(0);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -3292,6 +3322,11 @@ extern "C" int agb_dev_create(const agb_dev_desc *d, agb_dev **out) {
                     &v.br, &v.brw, &v.dera, &v.q2ab, &v.abrw, &v.deru, &v.derv, &v.derh, &v.derus, &v.dervs,
                     &v.o_sp, &v.o_br, &v.o_sa};
   for (size_t k = 0; k < sizeof(dbl) / sizeof(dbl[0]); k++) DALLOC(*dbl[k], N, double);
+  {
+    void *p;
+    if (dev_alloc(s, &p, (size_t)N * 80)) return -1; /* sizeof(TdAtom<double>) */
+    v.tdat = p;
+  }
   DALLOC(v.g_gb, 3 * N, double);
   DALLOC(v.g_vw, 3 * N, double);
   DALLOC(v.g_cav, 3 * N, double);
@@ -3813,7 +3848,7 @@ static void launch_all(agb_dev *s, int seg = -1) {
   }
   if (seg < 0) shard_allreduce(s, 2, st);
   if (seg < 0 || seg == 3) {
-  AGB_LAUNCH(k_gbders_post, nblocks(N), BLK, st, v);
+  AGB_LAUNCH(k_gbders_post<R>, nblocks(N), BLK, st, v);
   nl += 1;
   stage_mark(s, 7);
   if (side) {
