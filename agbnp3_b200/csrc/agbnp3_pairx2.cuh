@@ -117,11 +117,10 @@ __device__ __forceinline__ void agb_tile_x2(const AxI &I, AxP &P, AxJ &J, const 
   }
 }
 
-/* 116 registers: four resident blocks per SM (five, at 96 registers with
-   spills, measured 2 % slower) */
-/* one block of up to 16 warps per SM, whose warps take the items from a
-   device counter (spread over the list by take_unit): 2-6 % faster than
-   four 4-warp blocks per SM taking items in grid order */
+/* 115 registers, one block of up to 16 warps per SM, whose warps take the
+   items from a device counter (spread over the list by take_unit): 2-6 %
+   faster than four 4-warp blocks per SM taking items in grid order (five
+   such blocks, at 96 registers with spills, measured 2 % slower still) */
 __global__ void __launch_bounds__(512, 1) k_agb_x2(View v, const int4 *__restrict__ items, int nitems) {
   __shared__ float4 sjt[16][3][32];
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
